@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark: batched generalized eigensolves H u = lambda S u (complex128).
+
+One step = one sunny_geneig_launch over the whole batch (default N=54,
+batch 65,536, the baseline generator with cond(S) <= 100), inputs resident
+in HBM (6.1 GB of H and S, far larger than the 126 MB L2, so no flush is
+needed between steps). Prints ONE JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--n 54] [--batch 65536]
+  python bench.py --impl reference ...   # LAPACK zhegv on the host cores
+
+Multi-GPU (torchrun, one process per GPU): every rank solves its own
+batch (weak scaling, replicas; the path has no exchange step), the timed
+region is bracketed by barriers and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "N=54 gen-eig solves/s at ≤1e-12 residual, FP64 vs mixed; serving p50/p99 ms"
+
+
+def flops_per_solve(n: int) -> float:
+    # potrf 4/3 n^3 + hegst 4 n^3 + hetrd 16/3 n^3 + unmtr 8 n^3 + back-trsm 4 n^3 (real flops)
+    return 68.0 / 3.0 * n ** 3
+
+
+def hbm_bytes_per_solve(n: int) -> int:
+    # read H, S; write U (16 B each), W (8 B), info (4 B)
+    return 48 * n * n + 8 * n + 4
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--n", type=int, default=54)
+    p.add_argument("--batch", type=int, default=65536)
+    p.add_argument("--kappa", type=float, default=100.0)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--e2e-chunk", type=int, default=8192)
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle.cpu_baseline import ZhegvPool
+    per_worker = 16
+    pool = ZhegvPool(args.n, per_worker=per_worker, kappa=args.kappa)
+    try:
+        for _ in range(max(args.warmup, 1)):
+            pool.step()
+        total, wall = 0, 0.0
+        for _ in range(args.steps):
+            s, t = pool.step()
+            total += s
+            wall += t
+    finally:
+        pool.close()
+    value = total / wall
+    cpu = {"value": value, "unit": "solves/s", "cores": pool.workers, "kind": "port",
+           "sample": (f"each step: {pool.workers} single-threaded LAPACK zhegv workers (scipy OpenBLAS) "
+                      f"solve their own {per_worker} seeded N={args.n} problems; {total} solves in {wall:.2f} s")}
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, world),
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference's GPU paths need NVIDIA MathDx/cuSolverDx, absent offline; its own CPU "
+                 "ground truth (LAPACK zhegv) is timed instead"),
+    }
+    print(json.dumps(out), flush=True)
+
+
+def workload_config(args, world):
+    return {
+        "workload": (f"N={args.n} complex128 Hermitian-definite pairs, batch {args.batch} per GPU, "
+                     f"BdG-structured H (lambda_min = 0.1 ||H||), S = Q diag(d) Q^H with cond(S) <= "
+                     f"{args.kappa:g}; one launch per step"),
+        "n": args.n, "batch_per_gpu": args.batch, "global_batch": args.batch * world,
+        "cond_S_max": args.kappa, "parallelism": f"replicas x{world}",
+        "l2": "inputs 2 x batch x N^2 x 16 B >> 126 MB L2 (no flush needed)"
+        if 2 * args.batch * args.n * args.n * 16 > 126e6 else "inputs fit L2: L2 flushed between steps",
+    }
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd[1:1] = ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = sorted(r[0] for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- our arm
+def measure_fp64_peak(torch, dev) -> float:
+    """cuBLAS DGEMM TFLOP/s (torch.matmul float64, 8192^3), best of 4."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(); torch.matmul(a, b); e.record(); e.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle.cpu_baseline import time_zhegv   # CPU baseline leg (spawned before any CUDA use)
+        cpu = time_zhegv(args.n, per_worker=32, seconds=8.0, kappa=args.kappa)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from sunny_gen_eigensolver_b200 import Solver
+    from sunny_gen_eigensolver_b200.generators import baseline_problems_torch
+
+    n, batch = args.n, args.batch
+    H, S = baseline_problems_torch(n, batch, seed=20261203 + 1 + rank, kappa=args.kappa, device=dev)
+    H = H.transpose(-1, -2).contiguous()   # column-major buffers (Julia layout)
+    S = S.transpose(-1, -2).contiguous()
+    W = torch.empty((batch, n), dtype=torch.float64, device=dev)
+    U = torch.empty((batch, n, n), dtype=torch.complex128, device=dev)
+    info = torch.empty((batch,), dtype=torch.int32, device=dev)
+    solver = Solver(n, device_id=local)
+    stream = torch.cuda.current_stream(dev)
+
+    peak = measure_fp64_peak(torch, dev)
+
+    def barrier():
+        if world > 1:
+            t = torch.zeros(1, device=dev)
+            dist.all_reduce(t)
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        solver.launch(H, S, W, U, info, stream)
+    barrier()
+    props = torch.cuda.get_device_properties(dev)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None)
+    with ClockSampler(uuid) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            solver.launch(H, S, W, U, info, stream)
+        t1.record(stream)
+        barrier()
+    elapsed = t0.elapsed_time(t1) * 1e-3
+    el_t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
+    elapsed_max = float(el_t.item())
+    clocks = clk.summary()
+
+    # accuracy of the last step's results (all matrices, on the device)
+    bad = int((info != 0).sum().item())
+    Hn, Sn, Un = H.transpose(-1, -2), S.transpose(-1, -2), U.transpose(-1, -2)
+    R = Hn @ Un - (Sn @ Un) * W[:, None, :].to(torch.complex128)
+    hnorm_lb = torch.linalg.matrix_norm(Hn) / n ** 0.5        # ||H||_F / sqrt(n) <= ||H||_2
+    unorm_lb = torch.linalg.matrix_norm(Un) / n ** 0.5        # ||U||_F / sqrt(n) <= ||U||_2
+    res = torch.linalg.matrix_norm(R) / (hnorm_lb * unorm_lb)
+    G = Un.conj().transpose(-1, -2) @ Sn @ Un - torch.eye(n, dtype=torch.complex128, device=dev)
+    orth = G.abs().amax(dim=(-2, -1))
+    acc = {"max_residual_upper_bound": float(res.max().item()), "max_s_orth": float(orth.max().item()),
+           "failed_matrices": bad, "sorted": bool((W[:, 1:] >= W[:, :-1]).all().item())}
+    del R, G, res, orth
+
+    solves = batch * world * args.steps
+    value = solves / elapsed_max
+    per_launch = elapsed / args.steps
+    achieved = flops_per_solve(n) * batch / per_launch / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul (best of 4)",
+                "traffic": None,
+                "algorithmic_bytes_per_launch": hbm_bytes_per_solve(n) * batch,
+                "achieved_hbm_gbs": hbm_bytes_per_solve(n) * batch / per_launch / 1e9}
+    tfile = REPO / "profiles" / f"dram_traffic_n{n}.json"
+    if tfile.exists():
+        try:
+            t = json.loads(tfile.read_text())
+            roofline["traffic"] = t["dram_bytes_per_solve"] * batch
+            roofline["traffic_source"] = t.get("source", str(tfile.name))
+        except Exception:
+            pass
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, torch, solver, H, S, W, U, info, dev, world, dist)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded BdG H / Haar-unitary S generator, generated on the device)",
+            "config": workload_config(args, world),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": args.steps, "accuracy": acc,
+            "solver": {"regime": solver.regime, "block_dim_x": solver.block_dim_x,
+                       "shared_mem_bytes": solver.shared_mem_bytes, "path": solver.path_name},
+        }
+        print(json.dumps(out), flush=True)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_e2e(args, torch, solver, H, S, W, U, info, dev, world, dist):
+    """Same metric through the C ABI with HOST buffers: every step copies H and
+    S in from pinned host memory and W, U, info back out, pipelined in chunks
+    over three streams (H2D, launch and D2H of different chunks overlap)."""
+    batch, n = args.batch, args.n
+    Hh = H.cpu().pin_memory()
+    Sh = S.cpu().pin_memory()
+    Wh = torch.empty(W.shape, dtype=W.dtype).pin_memory()
+    Uh = torch.empty(U.shape, dtype=U.dtype).pin_memory()
+    ih = torch.empty(info.shape, dtype=info.dtype).pin_memory()
+    streams = [torch.cuda.Stream(dev) for _ in range(3)]
+    chunk = args.e2e_chunk
+
+    def step():
+        for k, off in enumerate(range(0, batch, chunk)):
+            sl = slice(off, min(batch, off + chunk))
+            s = streams[k % len(streams)]
+            with torch.cuda.stream(s):
+                H[sl].copy_(Hh[sl], non_blocking=True)
+                S[sl].copy_(Sh[sl], non_blocking=True)
+                solver.launch(H[sl], S[sl], W[sl], U[sl], info[sl], s)
+                Wh[sl].copy_(W[sl], non_blocking=True)
+                Uh[sl].copy_(U[sl], non_blocking=True)
+                ih[sl].copy_(info[sl], non_blocking=True)
+
+    steps = max(3, args.steps // 2)
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    cur = torch.cuda.current_stream(dev)
+    ev0.record(cur)
+    for s in streams:
+        s.wait_stream(cur)
+    for _ in range(steps):
+        step()
+    for s in streams:
+        cur.wait_stream(s)
+    ev1.record(cur)
+    torch.cuda.synchronize(dev)
+    el = max(ev0.elapsed_time(ev1) * 1e-3, 1e-9)
+    el_t = torch.tensor([el], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
+    el = float(el_t.item())
+    bi = 2 * batch * n * n * 16
+    bo = batch * (n * n * 16 + n * 8 + 4)
+    return {"value": batch * world * steps / el, "unit": "solves/s", "h2d_bytes_per_step": bi,
+            "d2h_bytes_per_step": bo, "steps": steps, "chunk": chunk, "streams": len(streams),
+            "host_wall_s": time.perf_counter() - t0}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,155 @@
+/*
+ * sunny_geneig.h -- C ABI of libsunny_geneig.so, the B200 (sm_100a) batched
+ * complex Hermitian-definite generalized eigensolver  H u = lambda S u.
+ *
+ * Drop-in for the reference's src/common/c_api.h: every type, enum value and
+ * function signature below that carries a "replaces" note has the same name,
+ * argument meaning and error behaviour as the reference entry point it names.
+ * Entry points marked "extension" have no counterpart in the reference.
+ *
+ * Buffers (all device pointers passed as uintptr_t, caller-owned):
+ *   d_H, d_S : complex128, column-major N x N per matrix, batch-contiguous
+ *              (element (i,j) of matrix b at b*N*N + j*N + i). Read only.
+ *              H is read in full (both triangles); S only in its lower triangle.
+ *   d_W      : float64 N x batch; ascending eigenvalues of matrix b at b*N.
+ *   d_U      : complex128 N x N x batch; column k of matrix b is the eigenvector
+ *              for W[b*N + k], normalised so that U^H S U = I.
+ *   d_info   : int32[batch]; 0 on success; N + k when the leading minor of
+ *              order k of S is not positive definite (LAPACK zhegv convention);
+ *              k in [1, N] when the tridiagonal eigensolver did not converge.
+ *              W and U of a failed matrix are filled with NaN.
+ * Launches are asynchronous on `stream` (0 = legacy default stream); the
+ * library never synchronises the host inside a launch.
+ * Alignment: d_H, d_S, d_U 16-byte, d_W 8-byte, d_info 4-byte aligned.
+ */
+#ifndef SUNNY_GENEIG_H
+#define SUNNY_GENEIG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* replaces src/common/c_api.h:22 (opaque handle) */
+typedef struct sunny_geneig_solver* sunny_geneig_solver_t;
+
+/* replaces src/common/c_api.h:24-30 */
+typedef enum {
+    SUNNY_GENEIG_OK            =  0,
+    SUNNY_GENEIG_INVALID_ARG   = -1,
+    SUNNY_GENEIG_DEVICE_ERROR  = -2,
+    SUNNY_GENEIG_COMPILE_ERROR = -3,
+    SUNNY_GENEIG_LAUNCH_ERROR  = -4
+} sunny_geneig_status_t;
+
+/* replaces src/common/c_api.h:32-36. Kernels here are compiled ahead of
+ * time, so the cache mode only governs the on-disk launch-shape table. */
+typedef enum {
+    SUNNY_GENEIG_CACHE_AUTO    = 0,
+    SUNNY_GENEIG_CACHE_NODISK  = 1,
+    SUNNY_GENEIG_CACHE_NOCACHE = 2
+} sunny_geneig_cache_mode_t;
+
+/* replaces src/common/c_api.h:38-41 */
+typedef enum {
+    SUNNY_GENEIG_TUNING_SUGGESTED = 0,
+    SUNNY_GENEIG_TUNING_AUTOTUNE  = 1
+} sunny_geneig_tuning_mode_t;
+
+/* replaces src/common/c_api.h:43-46. UNIFIED and HYBRID both select the
+ * plain FP64 sm_100a kernel (no cuSolverDx / cuSOLVER / cuBLAS here).
+ * MIXED is an extension: FP32 tridiagonal stage plus FP64 refinement. */
+typedef enum {
+    SUNNY_GENEIG_KERNEL_UNIFIED = 0,
+    SUNNY_GENEIG_KERNEL_HYBRID  = 1,
+    SUNNY_GENEIG_KERNEL_MIXED   = 2
+} sunny_geneig_kernel_mode_t;
+
+/* replaces src/common/c_api.h:50-55 (impl c_api.cpp:76-107).
+ * Returns NULL on failure (message in sunny_geneig_last_error()).
+ * batches_per_block_request <= 0 selects automatically. */
+sunny_geneig_solver_t sunny_geneig_create(
+    int                         n,
+    int                         device_id,
+    int                         batches_per_block_request,
+    sunny_geneig_tuning_mode_t  tuning_mode,
+    sunny_geneig_cache_mode_t   cache_mode);
+
+/* replaces src/common/c_api.h:63-69 (impl c_api.cpp:109-137) */
+sunny_geneig_solver_t sunny_geneig_create_ex(
+    int                         n,
+    int                         device_id,
+    int                         batches_per_block_request,
+    sunny_geneig_tuning_mode_t  tuning_mode,
+    sunny_geneig_cache_mode_t   cache_mode,
+    sunny_geneig_kernel_mode_t  kernel_mode);
+
+/* replaces src/common/c_api.h:72 (impl c_api.cpp:139-145). NULL is a no-op. */
+void sunny_geneig_destroy(sunny_geneig_solver_t solver);
+
+/* replaces src/common/c_api.h:77-85 (impl c_api.cpp:147-186).
+ * INVALID_ARG for a NULL solver, batch_size < 0, a NULL or misaligned
+ * buffer with batch_size > 0; batch_size == 0 is a no-op returning OK;
+ * LAUNCH_ERROR when the CUDA launch itself fails. */
+sunny_geneig_status_t sunny_geneig_launch(
+    sunny_geneig_solver_t solver,
+    uintptr_t             d_H,
+    uintptr_t             d_S,
+    uintptr_t             d_W,
+    uintptr_t             d_U,
+    uintptr_t             d_info,
+    int                   batch_size,
+    uintptr_t             stream);
+
+/* replace src/common/c_api.h:88-91 (impl c_api.cpp:188-208).
+ * -1 (0 for shared_mem_bytes) when solver is NULL. */
+int          sunny_geneig_matrix_size      (sunny_geneig_solver_t solver);
+int          sunny_geneig_batches_per_block(sunny_geneig_solver_t solver);
+int          sunny_geneig_block_dim_x      (sunny_geneig_solver_t solver);
+unsigned int sunny_geneig_shared_mem_bytes (sunny_geneig_solver_t solver);
+
+/* replaces src/common/c_api.h:95 (impl c_api.cpp:210-212). Thread-local,
+ * never NULL, "" when no error was recorded on the calling thread. */
+const char*  sunny_geneig_last_error(void);
+
+/* replace src/common/c_api.h:100-101 (impl c_api.cpp:214-220).
+ * path_name: "unified", "hybrid" or "mixed" ("" for NULL). */
+const char*                sunny_geneig_path_name  (sunny_geneig_solver_t solver);
+sunny_geneig_kernel_mode_t sunny_geneig_kernel_mode(sunny_geneig_solver_t solver);
+
+/* ---- extensions (no counterpart in the reference's C ABI) ---------------- */
+
+/* Stage-wise launch for parity tests; the stages follow the reference's
+ * static kernels in src/geneig_fixed.cu:
+ *   stage 1: Cholesky only (chol_n54_kernel :106-132). U <- L (lower, upper
+ *            triangle zero). W untouched.
+ *   stage 2: reduction (geneig_reduce_n54_kernel :166-206). U <- C =
+ *            L^-1 H L^-H, full Hermitian matrix.
+ *   stage 3: reduction + eigensolve (geneig_reduce_eig_n54_kernel :247-300).
+ *            W <- ascending eigenvalues of C, U <- orthonormal eigenvectors V.
+ *   stage 4: the full solve, identical to sunny_geneig_launch. */
+sunny_geneig_status_t sunny_geneig_launch_stage(
+    sunny_geneig_solver_t solver,
+    int                   stage,
+    uintptr_t             d_H,
+    uintptr_t             d_S,
+    uintptr_t             d_W,
+    uintptr_t             d_U,
+    uintptr_t             d_info,
+    int                   batch_size,
+    uintptr_t             stream);
+
+/* Largest N this build accepts in sunny_geneig_create. */
+int sunny_geneig_max_matrix_size(void);
+
+/* Name of the execution regime chosen at create time, e.g. "smem-cta"
+ * (both matrices resident in one CTA's shared memory) or "l2-slot"
+ * (matrices in a per-CTA global-memory slot). "" for NULL. */
+const char* sunny_geneig_regime_name(sunny_geneig_solver_t solver);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* SUNNY_GENEIG_H */

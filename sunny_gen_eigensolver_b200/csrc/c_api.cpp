@@ -1,0 +1,236 @@
+// C ABI of libsunny_geneig.so (declared in include/sunny_geneig.h).
+//
+// Same contract as the reference's src/common/c_api.cpp: nothrow at the
+// boundary, exceptions and CUDA errors become status codes, the last message
+// is kept per thread, device pointers travel as uintptr_t. Behind it there is
+// no runtime compilation: the sm_100a kernels are compiled ahead of time and
+// `create` only picks a launch plan and reserves the scratch that plan needs.
+
+#include "sunny_geneig.h"
+#include "geneig_kernels.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <exception>
+#include <new>
+#include <string>
+
+struct sunny_geneig_solver {
+    int n = 0;
+    int device = 0;
+    sunny_geneig_kernel_mode_t mode = SUNNY_GENEIG_KERNEL_UNIFIED;
+    sunny_geneig_tuning_mode_t tuning = SUNNY_GENEIG_TUNING_SUGGESTED;
+    sunny_geneig_cache_mode_t cache = SUNNY_GENEIG_CACHE_AUTO;
+    int bpb = 1;
+    sgeig::PlainPlan plan;
+    void* scratch = nullptr;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+
+// Runs `fn` with `device` current on the calling thread and restores the
+// caller's current device afterwards.
+template <typename F>
+cudaError_t with_device(int device, F&& fn) {
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return e;
+    if (prev != device) {
+        e = cudaSetDevice(device);
+        if (e != cudaSuccess) return e;
+    }
+    e = fn();
+    if (prev != device) cudaSetDevice(prev);
+    return e;
+}
+
+bool aligned(uintptr_t p, uintptr_t a) { return (p % a) == 0; }
+
+sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
+                                  sunny_geneig_tuning_mode_t tuning,
+                                  sunny_geneig_cache_mode_t cache,
+                                  sunny_geneig_kernel_mode_t mode, const char* fn) {
+    clear_error();
+    if (n < 1 || n > sgeig::kMaxN) {
+        set_error(std::string(fn) + ": n=" + std::to_string(n) + " outside [1, " +
+                  std::to_string(sgeig::kMaxN) + "]");
+        return nullptr;
+    }
+    if (mode != SUNNY_GENEIG_KERNEL_UNIFIED && mode != SUNNY_GENEIG_KERNEL_HYBRID) {
+        set_error(std::string(fn) + ": unsupported kernel_mode " + std::to_string((int)mode));
+        return nullptr;
+    }
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        set_error(std::string(fn) + ": no CUDA device available (" +
+                  (e != cudaSuccess ? cudaGetErrorString(e) : "device count 0") + ")");
+        return nullptr;
+    }
+    if (device_id < 0 || device_id >= count) {
+        set_error(std::string(fn) + ": device_id " + std::to_string(device_id) + " out of range");
+        return nullptr;
+    }
+    sunny_geneig_solver* s = nullptr;
+    try {
+        s = new sunny_geneig_solver();
+    } catch (const std::bad_alloc&) {
+        set_error(std::string("out of memory in ") + fn);
+        return nullptr;
+    }
+    s->n = n;
+    s->device = device_id;
+    s->mode = mode;
+    s->tuning = tuning;
+    s->cache = cache;
+    s->bpb = 1;
+    (void)bpb_request;
+    std::string err;
+    e = with_device(device_id, [&]() -> cudaError_t {
+        if (!sgeig::plain_plan(n, device_id, &s->plan, &err)) return cudaErrorInvalidValue;
+        if (s->plan.scratch_bytes) {
+            cudaError_t ea = cudaMalloc(&s->scratch, s->plan.scratch_bytes);
+            if (ea != cudaSuccess) { err = std::string("cudaMalloc scratch: ") + cudaGetErrorString(ea); return ea; }
+        }
+        return cudaSuccess;
+    });
+    if (e != cudaSuccess) {
+        set_error(std::string(fn) + ": " + (err.empty() ? cudaGetErrorString(e) : err));
+        if (s->scratch) with_device(device_id, [&]() { return cudaFree(s->scratch); });
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
+sunny_geneig_status_t launch_impl(sunny_geneig_solver_t s, int stage, uintptr_t d_H, uintptr_t d_S,
+                                  uintptr_t d_W, uintptr_t d_U, uintptr_t d_info, int batch,
+                                  uintptr_t stream, const char* fn) {
+    clear_error();
+    if (!s) { set_error(std::string(fn) + ": solver is NULL"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (batch < 0) { set_error(std::string(fn) + ": batch_size < 0"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (stage < 1 || stage > 4) { set_error(std::string(fn) + ": stage must be 1..4"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (batch == 0) return SUNNY_GENEIG_OK;
+    if (!d_H || !d_S || !d_W || !d_U || !d_info) {
+        set_error(std::string(fn) + ": NULL device buffer");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (!aligned(d_H, 16) || !aligned(d_S, 16) || !aligned(d_U, 16) || !aligned(d_W, 8) || !aligned(d_info, 4)) {
+        set_error(std::string(fn) + ": misaligned device buffer (H, S, U need 16 B; W 8 B; info 4 B)");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    try {
+        cudaError_t e = with_device(s->device, [&]() {
+            return sgeig::plain_launch(s->plan, stage, reinterpret_cast<const void*>(d_H),
+                                       reinterpret_cast<const void*>(d_S), reinterpret_cast<double*>(d_W),
+                                       reinterpret_cast<void*>(d_U), reinterpret_cast<int*>(d_info), batch,
+                                       s->scratch, reinterpret_cast<cudaStream_t>(stream));
+        });
+        if (e != cudaSuccess) {
+            set_error(std::string(fn) + ": kernel launch failed: " + cudaGetErrorString(e));
+            return SUNNY_GENEIG_LAUNCH_ERROR;
+        }
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return SUNNY_GENEIG_LAUNCH_ERROR;
+    } catch (...) {
+        set_error(std::string("unknown C++ exception in ") + fn);
+        return SUNNY_GENEIG_LAUNCH_ERROR;
+    }
+    return SUNNY_GENEIG_OK;
+}
+
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+sunny_geneig_solver_t sunny_geneig_create(int n, int device_id, int batches_per_block_request,
+                                          sunny_geneig_tuning_mode_t tuning_mode,
+                                          sunny_geneig_cache_mode_t cache_mode) {
+    try {
+        return create_impl(n, device_id, batches_per_block_request, tuning_mode, cache_mode,
+                           SUNNY_GENEIG_KERNEL_UNIFIED, "sunny_geneig_create");
+    } catch (...) {
+        set_error("unknown C++ exception in sunny_geneig_create");
+        return nullptr;
+    }
+}
+
+sunny_geneig_solver_t sunny_geneig_create_ex(int n, int device_id, int batches_per_block_request,
+                                             sunny_geneig_tuning_mode_t tuning_mode,
+                                             sunny_geneig_cache_mode_t cache_mode,
+                                             sunny_geneig_kernel_mode_t kernel_mode) {
+    try {
+        return create_impl(n, device_id, batches_per_block_request, tuning_mode, cache_mode, kernel_mode,
+                           "sunny_geneig_create_ex");
+    } catch (...) {
+        set_error("unknown C++ exception in sunny_geneig_create_ex");
+        return nullptr;
+    }
+}
+
+void sunny_geneig_destroy(sunny_geneig_solver_t solver) {
+    if (!solver) return;
+    try {
+        if (solver->scratch) {
+            const int dev = solver->device;
+            void* p = solver->scratch;
+            with_device(dev, [&]() { return cudaFree(p); });
+        }
+        delete solver;
+    } catch (...) {
+    }
+}
+
+sunny_geneig_status_t sunny_geneig_launch(sunny_geneig_solver_t solver, uintptr_t d_H, uintptr_t d_S,
+                                          uintptr_t d_W, uintptr_t d_U, uintptr_t d_info, int batch_size,
+                                          uintptr_t stream) {
+    return launch_impl(solver, 4, d_H, d_S, d_W, d_U, d_info, batch_size, stream, "sunny_geneig_launch");
+}
+
+sunny_geneig_status_t sunny_geneig_launch_stage(sunny_geneig_solver_t solver, int stage, uintptr_t d_H,
+                                                uintptr_t d_S, uintptr_t d_W, uintptr_t d_U, uintptr_t d_info,
+                                                int batch_size, uintptr_t stream) {
+    return launch_impl(solver, stage, d_H, d_S, d_W, d_U, d_info, batch_size, stream,
+                       "sunny_geneig_launch_stage");
+}
+
+int sunny_geneig_matrix_size(sunny_geneig_solver_t solver) { return solver ? solver->n : -1; }
+int sunny_geneig_batches_per_block(sunny_geneig_solver_t solver) { return solver ? solver->bpb : -1; }
+int sunny_geneig_block_dim_x(sunny_geneig_solver_t solver) { return solver ? solver->plan.threads : -1; }
+unsigned int sunny_geneig_shared_mem_bytes(sunny_geneig_solver_t solver) {
+    return solver ? static_cast<unsigned int>(solver->plan.smem) : 0u;
+}
+
+const char* sunny_geneig_last_error(void) { return g_last_error.c_str(); }
+
+const char* sunny_geneig_path_name(sunny_geneig_solver_t solver) {
+    if (!solver) return "";
+    switch (solver->mode) {
+        case SUNNY_GENEIG_KERNEL_HYBRID: return "hybrid";
+        case SUNNY_GENEIG_KERNEL_MIXED:  return "mixed";
+        default:                         return "unified";
+    }
+}
+
+sunny_geneig_kernel_mode_t sunny_geneig_kernel_mode(sunny_geneig_solver_t solver) {
+    if (!solver) return static_cast<sunny_geneig_kernel_mode_t>(-1);
+    return solver->mode;
+}
+
+int sunny_geneig_max_matrix_size(void) { return sgeig::kMaxN; }
+
+const char* sunny_geneig_regime_name(sunny_geneig_solver_t solver) {
+    if (!solver) return "";
+    return solver->plan.regime == sgeig::Regime::SmemCta ? "smem-cta" : "l2-slot";
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,43 @@
+// Internal launcher interface between the C ABI shim (c_api.cpp) and the
+// sm_100a kernels. Not installed; callers use include/sunny_geneig.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <string>
+
+namespace sgeig {
+
+// Largest N accepted at create time.
+constexpr int kMaxN = 512;
+// Largest N whose two working matrices fit one CTA's shared memory.
+int smem_cta_max_n();
+
+// How one solve is laid out on the device.
+enum class Regime : int {
+    SmemCta = 0,   // S->L and H->C->V->U resident in one CTA's shared memory
+    L2Slot  = 1,   // both matrices in a per-CTA global-memory slot (L2 resident)
+};
+
+struct PlainPlan {
+    int    n        = 0;
+    int    ld       = 0;      // leading dimension of the working matrices (odd)
+    int    threads  = 0;      // CTA size
+    size_t smem     = 0;      // dynamic shared memory per CTA
+    Regime regime   = Regime::SmemCta;
+    int    slots    = 0;      // L2Slot: number of resident CTAs (= scratch slots)
+    size_t scratch_bytes = 0; // L2Slot: bytes of device scratch needed
+};
+
+// Picks the regime and launch shape for size n on `device` and sets the
+// kernel attributes it needs. Returns false with a message on failure.
+bool plain_plan(int n, int device, PlainPlan* plan, std::string* err);
+
+// Enqueues one launch of `stage` (1..4) over `batch` matrices on `stream`.
+// `scratch` must hold plan.scratch_bytes when plan.regime == L2Slot.
+cudaError_t plain_launch(const PlainPlan& plan, int stage,
+                         const void* H, const void* S, double* W, void* U,
+                         int* info, long long batch, void* scratch,
+                         cudaStream_t stream);
+
+}  // namespace sgeig

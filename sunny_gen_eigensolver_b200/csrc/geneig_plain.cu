@@ -1,0 +1,444 @@
+// Plain FP64 batched generalized Hermitian-definite eigensolver for sm_100a.
+//
+// One CTA solves one matrix pair at a time (persistent over the batch):
+//   a1  load S -> A, H^H -> B                     (kernel_source.hpp:233-242)
+//   a2  A <- L, S = L L^H (lower Cholesky)        (:244)
+//   a3  B <- L^-1 H                               (:246)
+//   a4  B <- B L^-H = C   (done as L^-1 (L^-1 H)^H, same value)  (:248)
+//   a5  C = Q T Q^H (Householder, lower), T = Z diag(w) Z^T by implicit QL/QR,
+//       V = Q Z                                   (:250)
+//   a6  U = L^-H V                                (:252)
+//   a7  store W (ascending) and U                 (:268-276)
+// Column work (a3, a4, a6 and the back-transform of a5) is owned by groups
+// of G = 4 lanes per column, which synchronise with warp shuffles only; the
+// Cholesky and Householder steps use CTA barriers.
+//
+// Regimes: SmemCta keeps A and B (each n x ld complex, ld odd so that row
+// walks are bank-conflict free) in dynamic shared memory; L2Slot keeps them
+// in a per-CTA global-memory slot and only the vectors in shared memory.
+
+#include "geneig_common.cuh"
+#include "geneig_kernels.h"
+
+#include <cmath>
+#include <cstdio>
+
+namespace sgeig {
+namespace {
+
+constexpr int kG  = 4;     // lanes per column group
+constexpr int kNT = 256;   // threads per CTA
+
+struct PlainArgs {
+    const double2* __restrict__ H;
+    const double2* __restrict__ S;
+    double*  W;
+    double2* U;
+    int*     info;
+    double2* scratch;
+    long long batch;
+    int n, ld, stage;
+};
+
+// Shared-memory vector area (after the matrices in the SmemCta regime).
+struct VecArea {
+    double2* tau;   // n   Householder scalars
+    double2* vb;    // n   current Householder vector (v[k+1] = 1)
+    double2* pb;    // n   tau * A22 * v
+    double2* red;   // 32  reduction scratch
+    double*  d;     // n   tridiagonal diagonal / eigenvalues
+    double*  e;     // n   tridiagonal off-diagonal
+    double*  rdg;   // n   1 / L_kk
+    double*  rc;    // n   rotation cosines of the current sweep
+    double*  rs;    // n   rotation sines of the current sweep
+    int*     rank;  // n   ascending position of eigenvalue j
+    int*     ctl;   // 8   control words
+};
+
+__host__ __device__ inline size_t vec_area_bytes(int n) {
+    return (size_t)n * 16 * 3 + 32 * 16 + (size_t)n * 8 * 5 + (size_t)n * 4 + 8 * 4;
+}
+
+__device__ inline VecArea carve(unsigned char* p, int n) {
+    VecArea v;
+    v.tau = reinterpret_cast<double2*>(p);
+    v.vb  = v.tau + n;
+    v.pb  = v.vb + n;
+    v.red = v.pb + n;
+    v.d   = reinterpret_cast<double*>(v.red + 32);
+    v.e   = v.d + n;
+    v.rdg = v.e + n;
+    v.rc  = v.rdg + n;
+    v.rs  = v.rc + n;
+    v.rank = reinterpret_cast<int*>(v.rs + n);
+    v.ctl  = v.rank + n;
+    return v;
+}
+
+// X <- L^-1 X for the columns of X owned by this group (rows split by lane).
+__device__ __forceinline__ void group_forward_solve(const double2* A, const double* rdg, double2* X,
+                                                    int n, int ld, int g, int q, unsigned gmask) {
+    constexpr int NG = kNT / kG;
+    for (int j = g; j < n; j += NG) {
+        double2* x = X + (size_t)j * ld;
+        for (int k = 0; k < n; ++k) {
+            double2 xk = c2(0.0, 0.0);
+            const int owner = k % kG;
+            if (q == owner) { xk = cscale(x[k], rdg[k]); x[k] = xk; }
+            xk = group_bcast2<kG>(gmask, xk, owner);
+            const double2* lk = A + (size_t)k * ld;
+            for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) x[i] = cfms(x[i], lk[i], xk);
+        }
+    }
+}
+
+template <bool kL2Slot>
+__global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, ld = a.ld;
+    const size_t mat = (size_t)n * ld;
+
+    double2* A;
+    double2* B;
+    unsigned char* vec_base;
+    if (kL2Slot) {
+        A = a.scratch + (size_t)blockIdx.x * 2 * mat;
+        B = A + mat;
+        vec_base = smem_raw;
+    } else {
+        A = reinterpret_cast<double2*>(smem_raw);
+        B = A + mat;
+        vec_base = reinterpret_cast<unsigned char*>(B + mat);
+    }
+    VecArea v = carve(vec_base, n);
+
+    const int tid  = threadIdx.x;
+    const int g    = tid / kG;
+    const int q    = tid % kG;
+    const int lane = tid & 31;
+    const unsigned gmask = ((1u << kG) - 1u) << (lane & ~(kG - 1));
+    constexpr int NG = kNT / kG;
+    const size_t nn = (size_t)n * n;
+
+    for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) {
+        const double2* Hb = a.H + (size_t)b * nn;
+        const double2* Sb = a.S + (size_t)b * nn;
+        double*  Wb = a.W + (size_t)b * n;
+        double2* Ub = a.U + (size_t)b * nn;
+
+        __syncthreads();  // previous matrix fully consumed
+        // ---- a1: load. A(i,j) = S(i,j); B(i,j) = conj(H(j,i)), so that
+        // L^-1 (L^-1 H^H)^H = L^-1 H L^-H for any H (reads both triangles).
+        for (int idx = tid; idx < (int)nn; idx += kNT) {
+            const int j = idx / n, i = idx - j * n;
+            A[i + (size_t)j * ld] = __ldg(Sb + idx);
+            const double2 h = __ldg(Hb + idx);
+            B[j + (size_t)i * ld] = cconj(h);
+        }
+        if (tid < 8) v.ctl[tid] = 0;
+        __syncthreads();
+
+        // ---- a2: Cholesky (lower). Column k is finalised by its owner group,
+        // then every group applies it to the columns it owns.
+        for (int k = 0; k < n; ++k) {
+            if (k % NG == g) {
+                __syncwarp(gmask);
+                double2* ak = A + (size_t)k * ld;
+                const double akk = ak[k].x;
+                __syncwarp(gmask);          // every lane has read the pivot before it is overwritten
+                if (akk > 0.0) {            // false for NaN, as LAPACK's potrf test
+                    const double lk = sqrt(akk), r = 1.0 / lk;
+                    for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) ak[i] = cscale(ak[i], r);
+                    if (q == k % kG) { ak[k] = c2(lk, 0.0); v.rdg[k] = r; }
+                } else if (q == 0) {
+                    v.ctl[0] = k + 1;
+                }
+            }
+            __syncthreads();
+            if (v.ctl[0]) break;
+            const double2* ak = A + (size_t)k * ld;
+            int j = g;
+            while (j <= k) j += NG;
+            for (; j < n; j += NG) {
+                const double2 ljk = ak[j];
+                double2* aj = A + (size_t)j * ld;
+                for (int i = first_in_class<kG>(j, q); i < n; i += kG) aj[i] = cfms_bc(aj[i], ak[i], ljk);
+            }
+        }
+
+        int code = v.ctl[0] ? (n + v.ctl[0]) : 0;   // zhegv: info = n + order of failing minor
+        if (!code && a.stage >= 2) {
+            // ---- a3: B <- L^-1 H^H
+            group_forward_solve(A, v.rdg, B, n, ld, g, q, gmask);
+            __syncthreads();
+            // ---- a4: B <- L^-1 B^H  (= L^-1 H L^-H)
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                if (i > j) {
+                    const double2 x = B[i + (size_t)j * ld], y = B[j + (size_t)i * ld];
+                    B[i + (size_t)j * ld] = cconj(y);
+                    B[j + (size_t)i * ld] = cconj(x);
+                } else if (i == j) {
+                    B[i + (size_t)i * ld].y = -B[i + (size_t)i * ld].y;
+                }
+            }
+            __syncthreads();
+            group_forward_solve(A, v.rdg, B, n, ld, g, q, gmask);
+            __syncthreads();
+            // C is taken from its lower triangle, as a lower-fill heev does.
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                if (i > j) B[j + (size_t)i * ld] = cconj(B[i + (size_t)j * ld]);
+                else if (i == j) B[i + (size_t)i * ld].y = 0.0;
+            }
+            __syncthreads();
+        }
+
+        if (!code && a.stage >= 3) {
+            // ---- a5a: Householder tridiagonalisation (lower), C = Q T Q^H.
+            // Reflector k: H_k = I - tau_k v v^H on rows k+1..n-1, v[k+1] = 1.
+            // v[k+2..n) is kept in A's strict upper triangle, row k, and tau_k
+            // at A(k, k+1) (that triangle is unused by the Cholesky factor).
+            for (int k = 0; k < n - 1; ++k) {
+                double2* bk = B + (size_t)k * ld;
+                if (tid < 32) {
+                    double ss = 0.0;
+                    for (int i = k + 2 + tid; i < n; i += 32) { const double2 x = bk[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                    ss = warp_sum(ss);
+                    const double2 alpha = bk[k + 1];
+                    double2 taui, scal = c2(0.0, 0.0);
+                    double beta;
+                    if (ss == 0.0 && alpha.y == 0.0) {
+                        taui = c2(0.0, 0.0);
+                        beta = alpha.x;
+                    } else {
+                        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+                        taui = c2((beta - alpha.x) / beta, -alpha.y / beta);
+                        const double2 z = c2(alpha.x - beta, alpha.y);
+                        const double inv = 1.0 / (z.x * z.x + z.y * z.y);
+                        scal = c2(z.x * inv, -z.y * inv);
+                    }
+                    for (int i = k + 2 + tid; i < n; i += 32) {
+                        const double2 vi = cmul(bk[i], scal);
+                        v.vb[i] = vi;
+                        A[k + (size_t)i * ld] = vi;
+                    }
+                    if (tid == 0) {
+                        v.vb[k + 1] = c2(1.0, 0.0);
+                        v.tau[k] = taui;
+                        A[k + (size_t)(k + 1) * ld] = taui;
+                        v.d[k] = bk[k].x;
+                        v.e[k] = beta;
+                    }
+                }
+                __syncthreads();
+                const double2 taui = v.tau[k];
+                if (taui.x == 0.0 && taui.y == 0.0) continue;
+                // p = tau * A22 * v (A22 kept as a full Hermitian matrix)
+                for (int i = k + 1 + g; i < n; i += NG) {
+                    double2 acc = c2(0.0, 0.0);
+                    for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], v.vb[j]);
+                    acc = group_sum2<kG>(gmask, acc);
+                    if (q == 0) v.pb[i] = cmul(taui, acc);
+                }
+                __syncthreads();
+                if (tid < 32) {
+                    double2 dot = c2(0.0, 0.0);
+                    for (int i = k + 1 + tid; i < n; i += 32) dot = cfmac(dot, v.pb[i], v.vb[i]);
+                    dot = warp_sum2(dot);
+                    if (tid == 0) v.red[0] = cscale(cmul(taui, dot), -0.5);
+                }
+                __syncthreads();
+                const double2 alpha2 = v.red[0];
+                // A22 -= v w^H + w v^H,  w = p + alpha2 v
+                const int m = n - k - 1;
+                for (int idx = tid; idx < m * m; idx += kNT) {
+                    const int jj = idx / m, ii = idx - jj * m;
+                    const int i = k + 1 + ii, j = k + 1 + jj;
+                    const double2 vi = v.vb[i], vj = v.vb[j];
+                    const double2 wi = cfma(v.pb[i], alpha2, vi), wj = cfma(v.pb[j], alpha2, vj);
+                    double2 x = B[i + (size_t)j * ld];
+                    x = cfms_bc(x, vi, wj);
+                    x = cfms_bc(x, wi, vj);
+                    B[i + (size_t)j * ld] = x;
+                }
+                __syncthreads();
+            }
+            if (tid == 0) {
+                v.d[n - 1] = B[(n - 1) + (size_t)(n - 1) * ld].x;
+                if (n == 1) v.tau[0] = c2(0.0, 0.0);
+            }
+            // ---- a5b: Z = I (kept in the real parts of B), implicit QL/QR.
+            __syncthreads();
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                B[i + (size_t)j * ld] = c2(i == j ? 1.0 : 0.0, 0.0);
+            }
+            TridiagQL ql;
+            if (tid == 0) ql.init(n);
+            __syncthreads();
+            for (;;) {
+                if (tid == 0) {
+                    int lo = 0; bool backward = true;
+                    const int cnt = ql.next(v.d, v.e, v.rc, v.rs, lo, backward);
+                    v.ctl[1] = cnt; v.ctl[2] = lo; v.ctl[3] = backward ? 1 : 0;
+                    if (cnt == 0) v.ctl[4] = ql.info;
+                }
+                __syncthreads();
+                const int cnt = v.ctl[1];
+                if (cnt == 0) break;
+                const int lo = v.ctl[2];
+                const bool backward = v.ctl[3] != 0;
+                for (int i = tid; i < n; i += kNT) apply_sweep_row(B + i, ld, v.rc, v.rs, lo, cnt, backward);
+                __syncthreads();
+            }
+            if (v.ctl[4]) code = v.ctl[4];
+            // ascending rank of each eigenvalue (NaN ordered last)
+            if (!code) {
+                for (int j = tid; j < n; j += kNT) {
+                    const double dj = v.d[j];
+                    int r = 0;
+                    for (int k2 = 0; k2 < n; ++k2) {
+                        const double dk = v.d[k2];
+                        r += (dk < dj) || (dk == dj && k2 < j);
+                    }
+                    v.rank[j] = r;
+                }
+            }
+            __syncthreads();
+        }
+
+        // ---- outputs
+        if (code) {
+            const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+            for (int idx = tid; idx < (int)nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
+            if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
+            if (tid == 0) a.info[b] = code;
+            continue;
+        }
+        if (tid == 0) a.info[b] = 0;
+        if (a.stage == 1) {
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                Ub[idx] = (i >= j) ? A[i + (size_t)j * ld] : c2(0.0, 0.0);
+            }
+            continue;
+        }
+        if (a.stage == 2) {
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                Ub[idx] = B[i + (size_t)j * ld];
+            }
+            continue;
+        }
+        // a5c + a6 + a7, one column per group: V = Q Z, U = L^-H V, store.
+        for (int j = g; j < n; j += NG) {
+            double2* x = B + (size_t)j * ld;
+            for (int k = n - 2; k >= 0; --k) {
+                const double2 tk = v.tau[k];
+                if (tk.x == 0.0 && tk.y == 0.0) continue;
+                const double2* vk = A + k;   // v_k[i] = vk[i * ld] for i >= k+2
+                double2 s = c2(0.0, 0.0);
+                for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
+                    const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                    s = cfmac(s, vi, x[i]);
+                }
+                s = group_sum2<kG>(gmask, s);
+                const double2 ts = cmul(tk, s);
+                for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
+                    const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                    x[i] = cfms(x[i], ts, vi);
+                }
+            }
+            if (a.stage >= 4) {
+                // L^H u = x, back substitution; (L^H)(k, i) = conj(L(i, k)).
+                for (int i = n - 1; i >= 0; --i) {
+                    double2 ui = c2(0.0, 0.0);
+                    const int owner = i % kG;
+                    if (q == owner) { ui = cscale(x[i], v.rdg[i]); x[i] = ui; }
+                    ui = group_bcast2<kG>(gmask, ui, owner);
+                    for (int k = q; k < i; k += kG) x[k] = cfmsc(x[k], A[i + (size_t)k * ld], ui);
+                    // cfmsc(acc, a, b) = acc - conj(a)*b with a = L(i,k)
+                }
+            }
+            const int r = v.rank[j];
+            double2* uo = Ub + (size_t)r * n;
+            for (int i = q; i < n; i += kG) uo[i] = x[i];
+            if (q == 0) Wb[r] = v.d[j];
+        }
+    }
+}
+
+int g_smem_optin = -1;
+
+}  // namespace
+
+int smem_cta_max_n() {
+    // largest n with 2*n*ld*16 + vectors <= 227 KB (ld = n | 1)
+    int best = 0;
+    for (int n = 1; n <= kMaxN; ++n) {
+        const int ld = n | 1;
+        const size_t bytes = (size_t)2 * n * ld * 16 + vec_area_bytes(n);
+        if (bytes <= 232448) best = n;
+    }
+    return best;
+}
+
+bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
+    if (n < 1 || n > kMaxN) {
+        *err = "matrix size out of range [1, " + std::to_string(kMaxN) + "]";
+        return false;
+    }
+    int optin = 0, sms = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return false; }
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return false; }
+    g_smem_optin = optin;
+
+    PlainPlan p;
+    p.n = n;
+    p.ld = n | 1;
+    p.threads = kNT;
+    const size_t smem_cta = (size_t)2 * n * p.ld * 16 + vec_area_bytes(n);
+    if (smem_cta <= (size_t)optin) {
+        p.regime = Regime::SmemCta;
+        p.smem = smem_cta;
+        e = cudaFuncSetAttribute(geneig_plain_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    } else {
+        p.regime = Regime::L2Slot;
+        p.smem = vec_area_bytes(n);
+        p.slots = 2 * sms;
+        p.scratch_bytes = (size_t)p.slots * 2 * n * p.ld * 16;
+        e = cudaFuncSetAttribute(geneig_plain_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    }
+    if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
+    *plan = p;
+    return true;
+}
+
+cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const void* S, double* W,
+                         void* U, int* info, long long batch, void* scratch, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    PlainArgs a;
+    a.H = static_cast<const double2*>(H);
+    a.S = static_cast<const double2*>(S);
+    a.W = W;
+    a.U = static_cast<double2*>(U);
+    a.info = info;
+    a.scratch = static_cast<double2*>(scratch);
+    a.batch = batch;
+    a.n = plan.n;
+    a.ld = plan.ld;
+    a.stage = stage;
+    if (plan.regime == Regime::SmemCta) {
+        const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
+        geneig_plain_kernel<false><<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
+    } else {
+        const long long grid = batch < plan.slots ? batch : plan.slots;
+        geneig_plain_kernel<true><<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace sgeig
