@@ -148,6 +148,12 @@ int sunny_geneig_max_matrix_size(void);
  * (matrices in a per-CTA global-memory slot). "" for NULL. */
 const char* sunny_geneig_regime_name(sunny_geneig_solver_t solver);
 
+/* Self-test of the device reciprocal the eigensolver uses in place of FP64
+ * division (hardware approximation + two Newton-Raphson steps):
+ * out[i] = 1 / x[i] for n device doubles, asynchronously on `stream`. */
+sunny_geneig_status_t sunny_geneig_selftest_reciprocal(uintptr_t d_x, uintptr_t d_out, int n,
+                                                       uintptr_t stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

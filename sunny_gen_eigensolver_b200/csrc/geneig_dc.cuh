@@ -1,0 +1,349 @@
+// Divide-and-conquer eigensolver for the real symmetric tridiagonal matrix
+// T = tridiag(e, d, e), one CTA, everything in shared memory.
+//
+// Method (Cuppen's divide and conquer with the Gu-Eisenstat correction, the
+// algorithm of LAPACK dstedc / dlaed0-dlaed4):
+//   * T is torn at every index k in [1, n): d[k-1] and d[k] each lose |e[k-1]|,
+//     so that T = blockdiag(T1', T2') + |e| v v^T with v = e_{k-1} + sign(e) e_k.
+//   * Leaves are 1x1 (Z = I). Blocks are merged bottom-up along a power-of-two
+//     tree: level `half` merges [a, a+half) with [a+half, a+2*half).
+//   * A merge forms z = (last row of Q1, sign(e) * first row of Q2)/sqrt(2),
+//     rho = 2|e|, deflates entries with rho|z_j| <= tol and pairs of nearly
+//     equal poles (Givens rotation of the two eigenvector columns), solves the
+//     secular equation 1 + rho sum_j z_j^2/(d_j - lambda) = 0 for the K
+//     remaining roots (one thread per root), recomputes z from the computed
+//     roots with Loewner's formula so that the new eigenvectors are orthogonal
+//     to working precision, and multiplies the old eigenvector columns by the
+//     K x K eigenvector matrix of the rank-one problem.
+// The secular solver is this file's own: each root is bracketed between its
+// two poles, measured from the nearer pole (so that every d_j - lambda is
+// formed without cancellation), and iterated with a two-pole rational model
+// (fit value and slope of the left and right partial sums at the current
+// point, solve the resulting quadratic), safeguarded by bisection.
+//
+// Output: Z (n x n, column slot j holds the eigenvector of w[j]); w[] in the
+// caller's units. Eigenvalues are not sorted here.
+#pragma once
+
+#include "geneig_common.cuh"
+
+namespace sgeig {
+
+struct DCShared {
+    double* Z;  int ldz;    // eigenvectors
+    double* U;  int ldu;    // K x K blocks of each merge at [a, a+K)^2
+    double* d;  double* e;  // tridiagonal (modified)
+    double* w;              // eigenvalue of column slot j
+    double* z;              // merge z-vector by column slot
+    double* dl;             // non-deflated poles [a, a+K)
+    double* zz;             // their z
+    double* zh;             // Loewner z-hat
+    double* rt;             // root offsets from their origin pole
+    int* org;               // origin pole (merge-local index) of each root
+    int* nd;                // non-deflated column slots [a, a+K)
+    int* perm;              // ascending order of the merge's eigenvalues
+    int* kcnt;              // K per merge, indexed by a
+    double* rho;            // rho per merge, indexed by a
+    double* scal;           // [0] = scale applied to T
+};
+
+// Number of doubles / ints of scratch DCShared needs for size n (excluding Z, U).
+__host__ __device__ inline int dc_vec_doubles(int n) { return 8 * n + 2; }
+__host__ __device__ inline int dc_vec_ints(int n) { return 4 * n; }
+
+// Root i (0-based) of 1 + rho sum_j zz_j^2 / (dl_j - x) = 0 with dl ascending,
+// rho > 0. Returns the offset tau of the root from pole `org`; the return
+// value is the number of iterations taken.
+__host__ __device__ inline int secular_root(int i, int K, const double* dl, const double* zz, double rho,
+                                            double& tau_out, int& org_out) {
+    if (K == 1) { org_out = 0; tau_out = rho * zz[0] * zz[0]; return 0; }
+    int o;
+    double lo, hi, tau;
+    if (i < K - 1) {
+        const double gap = dl[i + 1] - dl[i];
+        const double mid = 0.5 * gap;
+        double g = 1.0;
+        for (int j = 0; j < K; ++j) {
+            const double del = (dl[j] - dl[i]) - mid;
+            g += rho * zz[j] * (zz[j] * fast_rcp(del));
+        }
+        if (g >= 0.0) { o = i;     lo = 0.0;  hi = mid; tau = mid; }
+        else          { o = i + 1; lo = -mid; hi = 0.0; tau = -mid; }
+    } else {
+        double s = 0.0;
+        for (int j = 0; j < K; ++j) s += zz[j] * zz[j];
+        o = K - 1; lo = 0.0; hi = rho * s; tau = hi;
+    }
+    const double dlo = dl[o];
+    const double p = dl[i] - dlo;
+    const double q = (i < K - 1) ? dl[i + 1] - dlo : 0.0;
+    int it = 0;
+    for (; it < 80; ++it) {
+        double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0, erra = 0.0;
+        for (int j = 0; j < K; ++j) {
+            const double del = (dl[j] - dlo) - tau;
+            const double t = zz[j] * fast_rcp(del);
+            const double term = rho * zz[j] * t;
+            const double dterm = rho * t * t;
+            if (j <= i) { psi += term; dpsi += dterm; }
+            else        { phi += term; dphi += dterm; }
+            erra += fabs(term);
+        }
+        const double g = 1.0 + psi + phi;
+        const double err = kEps * (2.0 + 8.0 * erra + 3.0 * fabs(tau) * (dpsi + dphi));
+        if (fabs(g) <= err) break;
+        if (g < 0.0) lo = tau; else hi = tau;
+        if (hi - lo <= 2.0 * kEps * fmax(fabs(lo), fabs(hi))) break;
+        double tn;
+        if (i < K - 1) {
+            const double bpsi = dpsi * (p - tau) * (p - tau);
+            const double apsi = psi - dpsi * (p - tau);
+            const double bphi = dphi * (q - tau) * (q - tau);
+            const double aphi = phi - dphi * (q - tau);
+            const double c = 1.0 + apsi + aphi;
+            // c + bpsi/(p - x) + bphi/(q - x) = 0 in origin coordinates
+            // (one of p, q is 0, so p q = 0):
+            //   c x^2 - (c (p + q) + bpsi + bphi) x + (bpsi q + bphi p) = 0
+            const double B = -(c * (p + q) + bpsi + bphi);
+            const double C = bpsi * q + bphi * p;
+            tn = lo - 1.0;
+            if (c == 0.0) {
+                tn = -C / B;
+            } else {
+                double disc = B * B - 4.0 * c * C;
+                if (disc < 0.0) disc = 0.0;
+                const double qq = -0.5 * (B + copysign(sqrt(disc), B));
+                const double x1 = qq / c, x2 = (qq != 0.0) ? C / qq : x1;
+                tn = (x1 > lo && x1 < hi) ? x1 : x2;
+            }
+        } else {
+            const double bpsi = dpsi * (p - tau) * (p - tau);
+            const double apsi = psi - dpsi * (p - tau);
+            const double den = 1.0 + apsi;
+            tn = (den > 0.0) ? p + bpsi / den : lo - 1.0;
+        }
+        // converged when the model step is within a few ulps of the iterate
+        // (it may then round just outside the bracket)
+        if (fabs(tn - tau) <= 4.0 * kEps * fabs(tau)) {
+            if (tn > lo && tn < hi) tau = tn;
+            break;
+        }
+        if (!(tn > lo && tn < hi) || it >= 30) tn = 0.5 * (lo + hi);
+        if (tn == tau) break;
+        tau = tn;
+    }
+    tau_out = tau;
+    org_out = o;
+    return it;
+}
+
+// All NT threads of the CTA call this. n >= 1. On return Z, w hold the
+// eigen-decomposition of the tridiagonal (d, e) given on entry.
+template <int NT, int NMAX>
+__device__ void tridiag_dc(int n, DCShared s) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+
+    // ---- scale T by a power of two so that max |T_ij| is in [0.5, 1)
+    if (tid < 32) {
+        double mx = 0.0;
+        for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(s.d[i]));
+        for (int i = lane; i < n - 1; i += 32) mx = fmax(mx, fabs(s.e[i]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) {
+            int ex = 0;
+            double sc = 1.0;
+            if (mx > 0.0 && isfinite(mx)) { frexp(mx, &ex); sc = ldexp(1.0, -ex); }
+            s.scal[0] = sc;
+        }
+    }
+    __syncthreads();
+    const double sc = s.scal[0];
+    // ---- scale, tear at every split, leaves: Z = I, w = d
+    for (int i = tid; i < n; i += NT) {
+        double di = s.d[i] * sc;
+        if (i > 0) di -= fabs(s.e[i - 1] * sc);
+        if (i < n - 1) di -= fabs(s.e[i] * sc);
+        s.w[i] = di;
+    }
+    for (int i = tid; i < n - 1; i += NT) s.e[i] *= sc;
+    for (int idx = tid; idx < n * n; idx += NT) {
+        const int j = idx / n, i = idx - j * n;
+        s.Z[i + j * s.ldz] = (i == j) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+
+    for (int half = 1; half < n; half <<= 1) {
+        const int span = half << 1;
+        // ---- phase A: one warp per merge: z, order, deflation
+        for (int a = warp * span; a < n; a += NW * span) {
+            const int k = a + half;
+            if (k >= n) { if (lane == 0) s.kcnt[a] = 0; continue; }
+            const int b = min(a + span, n);
+            const int m = b - a;
+            const double er = s.e[k - 1];
+            if (er == 0.0) { if (lane == 0) s.kcnt[a] = 0; continue; }
+            const double sgn = er < 0.0 ? -1.0 : 1.0;
+            const double rho = 2.0 * fabs(er);
+            double zmax = 0.0, dmax = 0.0;
+            for (int j = a + lane; j < b; j += 32) {
+                const double zj = (j < k ? s.Z[(k - 1) + j * s.ldz] : sgn * s.Z[k + j * s.ldz]) * 0.70710678118654752440;
+                s.z[j] = zj;
+                zmax = fmax(zmax, fabs(zj));
+                dmax = fmax(dmax, fabs(s.w[j]));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                zmax = fmax(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+                dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+            }
+            const double tol = 8.0 * kEps * fmax(dmax, zmax);
+            for (int j = a + lane; j < b; j += 32) {
+                const double wj = order_key(s.w[j]);
+                int r = 0;
+                for (int t = a; t < b; ++t) {
+                    const double wt = order_key(s.w[t]);
+                    r += (wt < wj) || (wt == wj && t < j);
+                }
+                s.perm[a + r] = j;   // r in [0, m): the keys are totally ordered
+            }
+            __syncwarp();
+            // fast path: keep entries with rho|z| > tol, in ascending order
+            int base = 0;
+            for (int t0 = 0; t0 < m; t0 += 32) {
+                const int t = t0 + lane;
+                int j = -1;
+                bool keep = false;
+                if (t < m) { j = s.perm[a + t]; keep = rho * fabs(s.z[j]) > tol; }
+                const unsigned mask = __ballot_sync(0xffffffffu, keep);
+                const int pos = base + __popc(mask & ((1u << lane) - 1u));
+                if (keep) { s.nd[a + pos] = j; s.dl[a + pos] = s.w[j]; s.zz[a + pos] = s.z[j]; }
+                base += __popc(mask);
+            }
+            __syncwarp();
+            const int K0 = base;
+            bool close = false;
+            for (int p = 1 + lane; p < K0; p += 32) {
+                const double T = s.dl[a + p] - s.dl[a + p - 1];
+                const double zn = s.zz[a + p], zp = s.zz[a + p - 1];
+                close |= fabs(T) * fabs(zn * zp) <= tol * (zn * zn + zp * zp);
+            }
+            close = __any_sync(0xffffffffu, close);
+            if (close && lane == 0) {
+                // sequential deflation with rotations of nearly equal poles
+                int K = 0, pj = -1;
+                for (int t = 0; t < m; ++t) {
+                    const int nj = s.perm[a + t];
+                    if (!(rho * fabs(s.z[nj]) > tol)) continue;
+                    if (pj < 0) { pj = nj; continue; }
+                    const double T = s.w[nj] - s.w[pj];
+                    const double zn = s.z[nj], zp = s.z[pj];
+                    const double t2 = zn * zn + zp * zp;
+                    if (fabs(T) * fabs(zn * zp) <= tol * t2) {
+                        const double ta = sqrt(t2);
+                        const double c = zn / ta, sn = -zp / ta;
+                        s.z[nj] = ta; s.z[pj] = 0.0;
+                        for (int r = a; r < b; ++r) {
+                            const double x = s.Z[r + pj * s.ldz], y = s.Z[r + nj * s.ldz];
+                            s.Z[r + pj * s.ldz] = c * x + sn * y;
+                            s.Z[r + nj * s.ldz] = c * y - sn * x;
+                        }
+                        const double wp = s.w[pj], wn = s.w[nj];
+                        s.w[pj] = wp * c * c + wn * sn * sn;
+                        s.w[nj] = wp * sn * sn + wn * c * c;
+                        pj = nj;
+                    } else {
+                        s.nd[a + K] = pj; s.dl[a + K] = s.w[pj]; s.zz[a + K] = s.z[pj]; ++K;
+                        pj = nj;
+                    }
+                }
+                if (pj >= 0) { s.nd[a + K] = pj; s.dl[a + K] = s.w[pj]; s.zz[a + K] = s.z[pj]; ++K; }
+                s.kcnt[a] = K;
+                s.rho[a] = rho;
+            } else if (lane == 0) {
+                s.kcnt[a] = K0;
+                s.rho[a] = rho;
+            }
+        }
+        __syncthreads();
+        // ---- phase B: secular roots, one thread per root
+        for (int pidx = tid; pidx < n; pidx += NT) {
+            const int a = pidx - pidx % span;
+            if (a + half >= n) continue;
+            const int i = pidx - a, K = s.kcnt[a];
+            if (i >= K) continue;
+            double t; int o;
+            secular_root(i, K, s.dl + a, s.zz + a, s.rho[a], t, o);
+            s.rt[pidx] = t;
+            s.org[pidx] = o;
+        }
+        __syncthreads();
+        // ---- phase C: Loewner z-hat
+        for (int pidx = tid; pidx < n; pidx += NT) {
+            const int a = pidx - pidx % span;
+            if (a + half >= n) continue;
+            const int i = pidx - a, K = s.kcnt[a];
+            if (i >= K) continue;
+            const double* dl = s.dl + a;
+            const double dli = dl[i];
+            double W = (dli - dl[s.org[a + i]]) - s.rt[a + i];
+            for (int j = 0; j < K; ++j) {
+                if (j == i) continue;
+                const double del = (dli - dl[s.org[a + j]]) - s.rt[a + j];
+                W *= del * fast_rcp(dli - dl[j]);
+            }
+            s.zh[pidx] = copysign(sqrt(fmax(-W, 0.0)), s.zz[pidx]);
+        }
+        __syncthreads();
+        // ---- phase D: eigenvector columns of the rank-one problem, new eigenvalues
+        for (int pidx = tid; pidx < n; pidx += NT) {
+            const int a = pidx - pidx % span;
+            if (a + half >= n) continue;
+            const int j = pidx - a, K = s.kcnt[a];
+            if (j >= K) continue;
+            const double* dl = s.dl + a;
+            const double base = dl[s.org[a + j]], tj = s.rt[a + j];
+            double* ucol = s.U + a + (size_t)(a + j) * s.ldu;
+            double nrm = 0.0;
+            for (int l = 0; l < K; ++l) {
+                const double v = s.zh[a + l] * fast_rcp((dl[l] - base) - tj);
+                ucol[l] = v;
+                nrm = fma(v, v, nrm);
+            }
+            const double inv = rsqrt(nrm);
+            for (int l = 0; l < K; ++l) ucol[l] *= inv;
+            s.w[s.nd[a + j]] = base + tj;
+        }
+        __syncthreads();
+        // ---- phase E: Z(:, nd) <- Z(:, nd) * U, row-parallel (4 threads per row)
+        for (int p0 = 0; p0 < 4 * n; p0 += NT) {
+            const int pidx = p0 + tid;
+            const int r = pidx >> 2, part = pidx & 3;
+            const int a = (r < n) ? r - r % span : n;
+            const bool active = r < n && a + half < n && s.kcnt[a] > 0;
+            const int K = active ? s.kcnt[a] : 0;
+            double qrow[NMAX];
+#pragma unroll
+            for (int l = 0; l < NMAX; ++l) qrow[l] = (l < K) ? s.Z[r + s.nd[a + l] * s.ldz] : 0.0;
+            __syncwarp();
+            for (int j = part; j < K; j += 4) {
+                const double* ucol = s.U + a + (size_t)(a + j) * s.ldu;
+                double acc = 0.0;
+#pragma unroll
+                for (int l = 0; l < NMAX; ++l) {
+                    if (l >= K) break;
+                    acc = fma(qrow[l], ucol[l], acc);
+                }
+                s.Z[r + s.nd[a + j] * s.ldz] = acc;
+            }
+        }
+        __syncthreads();
+    }
+    // ---- back to the caller's units
+    const double inv = 1.0 / sc;
+    for (int i = tid; i < n; i += NT) s.w[i] *= inv;
+    __syncthreads();
+}
+
+}  // namespace sgeig

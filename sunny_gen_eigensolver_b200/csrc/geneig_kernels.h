@@ -25,6 +25,7 @@ struct PlainPlan {
     int    threads  = 0;      // CTA size
     size_t smem     = 0;      // dynamic shared memory per CTA
     Regime regime   = Regime::SmemCta;
+    int    nmax     = 0;      // SmemCta: compile-time row bound of the register arrays
     int    slots    = 0;      // L2Slot: number of resident CTAs (= scratch slots)
     size_t scratch_bytes = 0; // L2Slot: bytes of device scratch needed
 };

@@ -18,6 +18,7 @@
 // in a per-CTA global-memory slot and only the vectors in shared memory.
 
 #include "geneig_common.cuh"
+#include "geneig_dc.cuh"
 #include "geneig_kernels.h"
 
 #include <cmath>
@@ -53,10 +54,13 @@ struct VecArea {
     double*  rs;    // n   rotation sines of the current sweep
     int*     rank;  // n   ascending position of eigenvalue j
     int*     ctl;   // 8   control words
+    double*  dcd;   // divide-and-conquer doubles (dc_vec_doubles(n))
+    int*     dci;   // divide-and-conquer ints (dc_vec_ints(n))
 };
 
 __host__ __device__ inline size_t vec_area_bytes(int n) {
-    return (size_t)n * 16 * 3 + 32 * 16 + (size_t)n * 8 * 5 + (size_t)n * 4 + 8 * 4;
+    return (size_t)n * 16 * 3 + 32 * 16 + (size_t)n * 8 * 5 + (size_t)n * 4 + 8 * 4 +
+           (size_t)dc_vec_doubles(n) * 8 + (size_t)dc_vec_ints(n) * 4;
 }
 
 __device__ inline VecArea carve(unsigned char* p, int n) {
@@ -70,8 +74,10 @@ __device__ inline VecArea carve(unsigned char* p, int n) {
     v.rdg = v.e + n;
     v.rc  = v.rdg + n;
     v.rs  = v.rc + n;
-    v.rank = reinterpret_cast<int*>(v.rs + n);
+    v.dcd  = v.rs + n;
+    v.rank = reinterpret_cast<int*>(v.dcd + dc_vec_doubles(n));
     v.ctl  = v.rank + n;
+    v.dci  = v.ctl + 8;
     return v;
 }
 
@@ -92,8 +98,8 @@ __device__ __forceinline__ void group_forward_solve(const double2* A, const doub
     }
 }
 
-template <bool kL2Slot>
-__global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
+template <bool kL2Slot, int NMAX>
+__global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_plain_kernel(PlainArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = a.n, ld = a.ld;
     const size_t mat = (size_t)n * ld;
@@ -268,38 +274,59 @@ __global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
                 v.d[n - 1] = B[(n - 1) + (size_t)(n - 1) * ld].x;
                 if (n == 1) v.tau[0] = c2(0.0, 0.0);
             }
-            // ---- a5b: Z = I (kept in the real parts of B), implicit QL/QR.
             __syncthreads();
-            for (int idx = tid; idx < (int)nn; idx += kNT) {
-                const int j = idx / n, i = idx - j * n;
-                B[i + (size_t)j * ld] = c2(i == j ? 1.0 : 0.0, 0.0);
-            }
-            TridiagQL ql;
-            if (tid == 0) ql.init(n);
-            __syncthreads();
-            for (;;) {
+            if constexpr (!kL2Slot) {
+                // ---- a5b: divide and conquer on T; Z (real) and its merge
+                // workspace share B's storage, eigenvalues land in dcd[0..n).
+                DCShared dc;
+                dc.Z = reinterpret_cast<double*>(B); dc.ldz = ld;
+                dc.U = dc.Z + (size_t)n * ld;        dc.ldu = ld;
+                dc.d = v.d; dc.e = v.e;
+                dc.w = v.dcd; dc.z = dc.w + n; dc.dl = dc.z + n; dc.zz = dc.dl + n; dc.zh = dc.zz + n;
+                dc.rt = dc.zh + n; dc.rho = dc.rt + n; dc.scal = dc.rho + n;
+                dc.org = v.dci; dc.nd = dc.org + n; dc.perm = dc.nd + n; dc.kcnt = dc.perm + n;
+                tridiag_dc<kNT, NMAX>(n, dc);
                 if (tid == 0) {
-                    int lo = 0; bool backward = true;
-                    const int cnt = ql.next(v.d, v.e, v.rc, v.rs, lo, backward);
-                    v.ctl[1] = cnt; v.ctl[2] = lo; v.ctl[3] = backward ? 1 : 0;
-                    if (cnt == 0) v.ctl[4] = ql.info;
+                    bool bad = false;
+                    for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
+                    v.ctl[4] = bad ? n : 0;
                 }
                 __syncthreads();
-                const int cnt = v.ctl[1];
-                if (cnt == 0) break;
-                const int lo = v.ctl[2];
-                const bool backward = v.ctl[3] != 0;
-                for (int i = tid; i < n; i += kNT) apply_sweep_row(B + i, ld, v.rc, v.rs, lo, cnt, backward);
+                if (v.ctl[4]) code = v.ctl[4];
+            } else {
+                // ---- a5b: Z = I (kept in the real parts of B), implicit QL/QR.
+                for (int idx = tid; idx < (int)nn; idx += kNT) {
+                    const int j = idx / n, i = idx - j * n;
+                    B[i + (size_t)j * ld] = c2(i == j ? 1.0 : 0.0, 0.0);
+                }
+                TridiagQL ql;
+                if (tid == 0) ql.init(n);
                 __syncthreads();
+                for (;;) {
+                    if (tid == 0) {
+                        int lo = 0; bool backward = true;
+                        const int cnt = ql.next(v.d, v.e, v.rc, v.rs, lo, backward);
+                        v.ctl[1] = cnt; v.ctl[2] = lo; v.ctl[3] = backward ? 1 : 0;
+                        if (cnt == 0) v.ctl[4] = ql.info;
+                    }
+                    __syncthreads();
+                    const int cnt = v.ctl[1];
+                    if (cnt == 0) break;
+                    const int lo = v.ctl[2];
+                    const bool backward = v.ctl[3] != 0;
+                    for (int i = tid; i < n; i += kNT) apply_sweep_row(B + i, ld, v.rc, v.rs, lo, cnt, backward);
+                    __syncthreads();
+                }
+                if (v.ctl[4]) code = v.ctl[4];
+                for (int i = tid; i < n; i += kNT) v.dcd[i] = v.d[i];
             }
-            if (v.ctl[4]) code = v.ctl[4];
-            // ascending rank of each eigenvalue (NaN ordered last)
+            // ascending rank of each eigenvalue
             if (!code) {
                 for (int j = tid; j < n; j += kNT) {
-                    const double dj = v.d[j];
+                    const double dj = order_key(v.dcd[j]);
                     int r = 0;
                     for (int k2 = 0; k2 < n; ++k2) {
-                        const double dk = v.d[k2];
+                        const double dk = order_key(v.dcd[k2]);
                         r += (dk < dj) || (dk == dj && k2 < j);
                     }
                     v.rank[j] = r;
@@ -331,45 +358,122 @@ __global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
             }
             continue;
         }
-        // a5c + a6 + a7, one column per group: V = Q Z, U = L^-H V, store.
-        for (int j = g; j < n; j += NG) {
-            double2* x = B + (size_t)j * ld;
-            for (int k = n - 2; k >= 0; --k) {
-                const double2 tk = v.tau[k];
-                if (tk.x == 0.0 && tk.y == 0.0) continue;
-                const double2* vk = A + k;   // v_k[i] = vk[i * ld] for i >= k+2
-                double2 s = c2(0.0, 0.0);
-                for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
-                    const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
-                    s = cfmac(s, vi, x[i]);
+        if constexpr (!kL2Slot) {
+            // a5c + a6 + a7 in registers, one column per group (rows i = q + G t):
+            // x = Q z_j, then L^H u = x, then store u as column rank[j].
+            constexpr int R = NMAX / kG;
+            const double* Z = reinterpret_cast<const double*>(B);
+            for (int j = g; j < n; j += NG) {
+                double2 x[R];
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    const int i = q + kG * t;
+                    x[t] = c2(i < n ? Z[i + (size_t)j * ld] : 0.0, 0.0);
                 }
-                s = group_sum2<kG>(gmask, s);
-                const double2 ts = cmul(tk, s);
-                for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
-                    const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
-                    x[i] = cfms(x[i], ts, vi);
+                for (int k = n - 2; k >= 0; --k) {
+                    const double2 tk = v.tau[k];
+                    if (tk.x == 0.0 && tk.y == 0.0) continue;
+                    const double2* vk = A + k;   // v_k[i] = vk[i * ld] for i >= k+2, v_k[k+1] = 1
+                    double2 s = c2(0.0, 0.0);
+#pragma unroll
+                    for (int t = 0; t < R; ++t) {
+                        const int i = q + kG * t;
+                        if (i > k && i < n) {
+                            const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                            s = cfmac(s, vi, x[t]);
+                        }
+                    }
+                    s = group_sum2<kG>(gmask, s);
+                    const double2 ts = cmul(tk, s);
+#pragma unroll
+                    for (int t = 0; t < R; ++t) {
+                        const int i = q + kG * t;
+                        if (i > k && i < n) {
+                            const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                            x[t] = cfms(x[t], ts, vi);
+                        }
+                    }
                 }
+                if (a.stage >= 4) {
+                    // back substitution, row i = qq + G tt from the bottom up
+#pragma unroll
+                    for (int tt = R - 1; tt >= 0; --tt) {
+#pragma unroll
+                        for (int qq = kG - 1; qq >= 0; --qq) {
+                            const int i = qq + kG * tt;
+                            if (i >= n) continue;
+                            double2 ui = c2(0.0, 0.0);
+                            if (q == qq) { ui = cscale(x[tt], v.rdg[i]); x[tt] = ui; }
+                            ui = group_bcast2<kG>(gmask, ui, qq);
+#pragma unroll
+                            for (int t = 0; t <= tt; ++t) {
+                                const int kr = q + kG * t;
+                                if (kr < i) x[t] = cfmsc(x[t], A[i + (size_t)kr * ld], ui);
+                            }
+                        }
+                    }
+                }
+                const int r = v.rank[j];
+                double2* uo = Ub + (size_t)r * n;
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    const int i = q + kG * t;
+                    if (i < n) uo[i] = x[t];
+                }
+                if (q == 0) Wb[r] = v.dcd[j];
             }
-            if (a.stage >= 4) {
-                // L^H u = x, back substitution; (L^H)(k, i) = conj(L(i, k)).
-                for (int i = n - 1; i >= 0; --i) {
-                    double2 ui = c2(0.0, 0.0);
-                    const int owner = i % kG;
-                    if (q == owner) { ui = cscale(x[i], v.rdg[i]); x[i] = ui; }
-                    ui = group_bcast2<kG>(gmask, ui, owner);
-                    for (int k = q; k < i; k += kG) x[k] = cfmsc(x[k], A[i + (size_t)k * ld], ui);
-                    // cfmsc(acc, a, b) = acc - conj(a)*b with a = L(i,k)
+        } else {
+            // a5c + a6 + a7 in place in B, one column per group: V = Q Z, U = L^-H V.
+            for (int j = g; j < n; j += NG) {
+                double2* x = B + (size_t)j * ld;
+                for (int k = n - 2; k >= 0; --k) {
+                    const double2 tk = v.tau[k];
+                    if (tk.x == 0.0 && tk.y == 0.0) continue;
+                    const double2* vk = A + k;
+                    double2 s = c2(0.0, 0.0);
+                    for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
+                        const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                        s = cfmac(s, vi, x[i]);
+                    }
+                    s = group_sum2<kG>(gmask, s);
+                    const double2 ts = cmul(tk, s);
+                    for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
+                        const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                        x[i] = cfms(x[i], ts, vi);
+                    }
                 }
+                if (a.stage >= 4) {
+                    for (int i = n - 1; i >= 0; --i) {
+                        double2 ui = c2(0.0, 0.0);
+                        const int owner = i % kG;
+                        if (q == owner) { ui = cscale(x[i], v.rdg[i]); x[i] = ui; }
+                        ui = group_bcast2<kG>(gmask, ui, owner);
+                        for (int k = q; k < i; k += kG) x[k] = cfmsc(x[k], A[i + (size_t)k * ld], ui);
+                    }
+                }
+                const int r = v.rank[j];
+                double2* uo = Ub + (size_t)r * n;
+                for (int i = q; i < n; i += kG) uo[i] = x[i];
+                if (q == 0) Wb[r] = v.dcd[j];
             }
-            const int r = v.rank[j];
-            double2* uo = Ub + (size_t)r * n;
-            for (int i = q; i < n; i += kG) uo[i] = x[i];
-            if (q == 0) Wb[r] = v.d[j];
         }
     }
 }
 
 int g_smem_optin = -1;
+
+// Register-array bound of the shared-memory regime for size n.
+int nmax_for(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : 96); }
+
+using KernelFn = void (*)(PlainArgs);
+KernelFn kernel_for(Regime r, int nmax) {
+    if (r == Regime::L2Slot) return geneig_plain_kernel<true, 0>;
+    switch (nmax) {
+        case 32: return geneig_plain_kernel<false, 32>;
+        case 64: return geneig_plain_kernel<false, 64>;
+        default: return geneig_plain_kernel<false, 96>;
+    }
+}
 
 }  // namespace
 
@@ -401,17 +505,17 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
     p.ld = n | 1;
     p.threads = kNT;
     const size_t smem_cta = (size_t)2 * n * p.ld * 16 + vec_area_bytes(n);
-    if (smem_cta <= (size_t)optin) {
+    if (smem_cta <= (size_t)optin && n <= 96) {
         p.regime = Regime::SmemCta;
         p.smem = smem_cta;
-        e = cudaFuncSetAttribute(geneig_plain_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+        p.nmax = nmax_for(n);
     } else {
         p.regime = Regime::L2Slot;
         p.smem = vec_area_bytes(n);
         p.slots = 2 * sms;
         p.scratch_bytes = (size_t)p.slots * 2 * n * p.ld * 16;
-        e = cudaFuncSetAttribute(geneig_plain_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     }
+    e = cudaFuncSetAttribute(kernel_for(p.regime, p.nmax), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
     *plan = p;
     return true;
@@ -431,13 +535,9 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const 
     a.n = plan.n;
     a.ld = plan.ld;
     a.stage = stage;
-    if (plan.regime == Regime::SmemCta) {
-        const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
-        geneig_plain_kernel<false><<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
-    } else {
-        const long long grid = batch < plan.slots ? batch : plan.slots;
-        geneig_plain_kernel<true><<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
-    }
+    long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
+    if (plan.regime == Regime::L2Slot && grid > plan.slots) grid = plan.slots;
+    kernel_for(plan.regime, plan.nmax)<<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
     return cudaGetLastError();
 }
 
