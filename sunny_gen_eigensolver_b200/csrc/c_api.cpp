@@ -229,7 +229,11 @@ int sunny_geneig_max_matrix_size(void) { return sgeig::kMaxN; }
 
 const char* sunny_geneig_regime_name(sunny_geneig_solver_t solver) {
     if (!solver) return "";
-    return solver->plan.regime == sgeig::Regime::SmemCta ? "smem-cta" : "l2-slot";
+    switch (solver->plan.regime) {
+        case sgeig::Regime::SmemCta:  return "smem-cta";
+        case sgeig::Regime::SmemWide: return "smem-wide";
+        default:                      return "l2-slot";
+    }
 }
 
 }  // extern "C"

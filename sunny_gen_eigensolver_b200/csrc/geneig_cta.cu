@@ -1,0 +1,541 @@
+// Batched generalized Hermitian-definite eigensolver, shared-memory regime
+// (N <= 64): one 256-thread CTA holds one matrix pair in shared memory and
+// solves it end to end; CTAs are persistent over the batch.
+//
+// Stage chain (reference: src/unified/kernel_source.hpp:233-276):
+//   a1  load S -> A, H -> B                                   (:233-242)
+//   a2  Cholesky S = L L^H, right-looking, one barrier per column  (:244)
+//       then L^-1 in place (forward substitution on I, rows owned by
+//       groups of four lanes)
+//   a3+a4  C = L^-1 H L^-H as two register-tiled GEMMs with X = L^-1:
+//       T = H X^H, then C = X T (lower triangle kept and mirrored); H is
+//       read in full, as the reference's two triangular solves do (:246-248)
+//   a5  Householder tridiagonalisation (lower), divide and conquer on the
+//       tridiagonal, back-transform V = Q Z in registers per column (:250)
+//   a6  U = L^-H V as a register-tiled GEMM                    (:252)
+//   a7  W (ascending) and U, columns permuted by eigenvalue rank (:268-276)
+//
+// Thread layouts (NT = 256): a 16 x 16 grid (tr = tid / 16, tc = tid % 16)
+// owning TM x TM register tiles (rows tr + 16 a, columns tc + 16 b) for the
+// GEMMs and the Householder rank-2 updates; groups of four lanes
+// (g = tid / 4, q = tid % 4) owning one row or one column for the
+// substitutions and the back-transform.
+
+#include "geneig_common.cuh"
+#include "geneig_dc.cuh"
+#include "geneig_kernels.h"
+
+namespace sgeig {
+namespace {
+
+constexpr int kNT = 256;
+constexpr int kG = 4;
+constexpr int kNG = kNT / kG;
+
+struct CtaArgs {
+    const double2* __restrict__ H;
+    const double2* __restrict__ S;
+    double*  W;
+    double2* U;
+    int*     info;
+    long long batch;
+    int n, ld, stage;
+};
+
+struct CtaVec {
+    double2* tau;   // n   Householder scalars
+    double2* vb;    // n   current Householder vector
+    double2* pb;    // n   tau * A22 * v
+    double2* wred;  // 8   per-warp partial dots
+    double*  d;     // n
+    double*  e;     // n
+    double*  rdg;   // n   1 / L_kk
+    double*  dcd;   // D&C doubles
+    int*     dci;   // D&C ints
+    int*     rank;  // n
+    int*     ctl;   // 8
+};
+
+__host__ __device__ inline size_t cta_vec_bytes(int n) {
+    return (size_t)n * 16 * 3 + 8 * 16 + (size_t)n * 8 * 3 + (size_t)dc_vec_doubles(n) * 8 +
+           (size_t)dc_vec_ints(n) * 4 + (size_t)n * 4 + 8 * 4;
+}
+
+__device__ inline CtaVec cta_carve(unsigned char* p, int n) {
+    CtaVec v;
+    v.tau  = reinterpret_cast<double2*>(p);
+    v.vb   = v.tau + n;
+    v.pb   = v.vb + n;
+    v.wred = v.pb + n;
+    v.d    = reinterpret_cast<double*>(v.wred + 8);
+    v.e    = v.d + n;
+    v.rdg  = v.e + n;
+    v.dcd  = v.rdg + n;
+    v.dci  = reinterpret_cast<int*>(v.dcd + dc_vec_doubles(n));
+    v.rank = v.dci + dc_vec_ints(n);
+    v.ctl  = v.rank + n;
+    return v;
+}
+
+template <int TM>
+__device__ __forceinline__ void tile_zero(double2 (&acc)[TM][TM]) {
+#pragma unroll
+    for (int a = 0; a < TM; ++a)
+#pragma unroll
+        for (int b = 0; b < TM; ++b) acc[a][b] = c2(0.0, 0.0);
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(CtaArgs a) {
+    constexpr int TM = NMAX / 16;   // register tile edge
+    constexpr int R = NMAX / kG;    // rows per lane in a column group
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, ld = a.ld;
+    const size_t mat = (size_t)n * ld;
+    double2* A = reinterpret_cast<double2*>(smem_raw);
+    double2* B = A + mat;
+    CtaVec v = cta_carve(reinterpret_cast<unsigned char*>(B + mat), n);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tr = tid >> 4, tc = tid & 15;
+    const int g = tid >> 2, q = tid & 3;
+    const unsigned gmask = 0xFu << (lane & ~3);
+    const size_t nn = (size_t)n * n;
+
+    for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) {
+        const double2* Hb = a.H + (size_t)b * nn;
+        const double2* Sb = a.S + (size_t)b * nn;
+        double*  Wb = a.W + (size_t)b * n;
+        double2* Ub = a.U + (size_t)b * nn;
+
+        __syncthreads();
+        // ---- a1: load (rows by tc so that global reads are contiguous)
+        for (int j = tr; j < n; j += 16)
+            for (int i = tc; i < n; i += 16) {
+                A[i + (size_t)j * ld] = __ldg(Sb + i + (size_t)j * n);
+                B[i + (size_t)j * ld] = __ldg(Hb + i + (size_t)j * n);
+            }
+        if (tid < 8) v.ctl[tid] = 0;
+
+        // ---- a2: Cholesky, right-looking. Step k reads the unscaled column
+        // k (final after step k-1), updates the trailing lower triangle with
+        // a_ij -= a_ik conj(a_jk) / a_kk, and rescales column k-1 (no longer
+        // read by anyone) to L(:, k-1).
+        int fail = 0;
+        double rprev = 0.0;
+        for (int k = 0; k < n; ++k) {
+            __syncthreads();
+            const double akk = A[k + (size_t)k * ld].x;
+            if (!(akk > 0.0)) { fail = k + 1; break; }   // uniform: every thread reads akk
+            const double r = rsqrt(akk);
+            if (k > 0) {
+                const int c = k - 1;
+                for (int i = c + tid; i < n; i += kNT) {
+                    double2* p = A + i + (size_t)c * ld;
+                    *p = (i == c) ? c2(1.0 / rprev, 0.0) : cscale(*p, rprev);
+                }
+                if (tid == 0) v.rdg[c] = rprev;
+            }
+            const double r2 = r * r;
+            const double2* ak = A + (size_t)k * ld;
+            double2 li[TM], lj[TM];
+#pragma unroll
+            for (int t = 0; t < TM; ++t) {
+                const int i = k + 1 + tr + 16 * t, j = k + 1 + tc + 16 * t;
+                li[t] = (i < n) ? ak[i] : c2(0.0, 0.0);
+                lj[t] = (j < n) ? cscale(cconj(ak[j]), r2) : c2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int bb = 0; bb < TM; ++bb) {
+                const int j = k + 1 + tc + 16 * bb;
+                if (j >= n) break;
+                double2* aj = A + (size_t)j * ld;
+#pragma unroll
+                for (int aa = 0; aa < TM; ++aa) {
+                    const int i = k + 1 + tr + 16 * aa;
+                    if (i >= n) break;
+                    if (i >= j) aj[i] = cfms(aj[i], li[aa], lj[bb]);
+                }
+            }
+            rprev = r;
+        }
+        __syncthreads();
+        if (!fail) {
+            const int c = n - 1;
+            if (tid == 0) {
+                A[c + (size_t)c * ld] = c2(1.0 / rprev, 0.0);
+                v.rdg[c] = rprev;
+            }
+        }
+        __syncthreads();
+        int code = fail ? n + fail : 0;   // zhegv: info = n + order of the failing minor
+
+        if (!code && a.stage == 1) {
+            for (int j = tr; j < n; j += 16)
+                for (int i = tc; i < n; i += 16)
+                    Ub[i + (size_t)j * n] = (i >= j) ? A[i + (size_t)j * ld] : c2(0.0, 0.0);
+            if (tid == 0) a.info[b] = 0;
+            continue;
+        }
+
+        if (!code) {
+            // ---- L^-1 in place. Row k is finalised (X(k, j) = acc(k, j)/L_kk)
+            // by its own group, then every later row i subtracts
+            // L(i, k) X(k, :). acc(i, j) lives in the slot of L(i, j), whose
+            // last use is step j; at step k the slot (i, k) is overwritten with
+            // -L(i, k) X(k, k) after all four lanes of row i have read L(i, k).
+            for (int k = 0; k < n; ++k) {
+                if (g == k % kNG) {   // finalise row k (row i is always handled by group i % 64)
+                    const double rk = v.rdg[k];
+                    for (int j = q; j < k; j += kG) A[k + (size_t)j * ld] = cscale(A[k + (size_t)j * ld], rk);
+                    if (q == 0) A[k + (size_t)k * ld] = c2(rk, 0.0);
+                }
+                __syncthreads();
+                for (int i = g; i < n; i += kNG) {
+                    if (i <= k) continue;
+                    const double2 lik = A[i + (size_t)k * ld];
+                    __syncwarp(gmask);
+                    for (int j = q; j <= k; j += kG) {
+                        const double2 xkj = A[k + (size_t)j * ld];
+                        double2* p = A + i + (size_t)j * ld;
+                        *p = (j == k) ? cscale(cmul(lik, xkj), -1.0) : cfms(*p, lik, xkj);
+                    }
+                }
+            }
+            __syncthreads();
+            // A now holds X = L^-1 in its lower triangle (diagonal real).
+            // ---- a3: T = H X^H, T(i, j) = sum_{k <= j} H(i, k) conj(X(j, k))
+            {
+                double2 acc[TM][TM];
+                tile_zero<TM>(acc);
+                int kmax = tc + 16 * (TM - 1);
+                if (kmax > n - 1) kmax = n - 1;
+                for (int k = 0; k <= kmax; ++k) {
+                    double2 hv[TM], xv[TM];
+                    const double2* bk = B + (size_t)k * ld;
+#pragma unroll
+                    for (int t = 0; t < TM; ++t) {
+                        const int i = tr + 16 * t, j = tc + 16 * t;
+                        hv[t] = (i < n) ? bk[i] : c2(0.0, 0.0);
+                        xv[t] = (j < n && k <= j) ? cconj(A[j + (size_t)k * ld]) : c2(0.0, 0.0);
+                    }
+#pragma unroll
+                    for (int aa = 0; aa < TM; ++aa)
+#pragma unroll
+                        for (int bb = 0; bb < TM; ++bb) acc[aa][bb] = cfma(acc[aa][bb], hv[aa], xv[bb]);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int aa = 0; aa < TM; ++aa)
+#pragma unroll
+                    for (int bb = 0; bb < TM; ++bb) {
+                        const int i = tr + 16 * aa, j = tc + 16 * bb;
+                        if (i < n && j < n) B[i + (size_t)j * ld] = acc[aa][bb];
+                    }
+                __syncthreads();
+            }
+            // ---- a4: C = X T, C(i, j) = sum_{k <= i} X(i, k) T(k, j); keep the
+            // lower triangle and mirror it, so that C is exactly Hermitian.
+            {
+                double2 acc[TM][TM];
+                tile_zero<TM>(acc);
+                int kmax = tr + 16 * (TM - 1);
+                if (kmax > n - 1) kmax = n - 1;
+                for (int k = 0; k <= kmax; ++k) {
+                    double2 xv[TM], tv[TM];
+                    const double2* xk = A + (size_t)k * ld;
+                    const double2* tk = B + k;
+#pragma unroll
+                    for (int t = 0; t < TM; ++t) {
+                        const int i = tr + 16 * t, j = tc + 16 * t;
+                        xv[t] = (i < n && k <= i) ? xk[i] : c2(0.0, 0.0);
+                        tv[t] = (j < n) ? tk[(size_t)j * ld] : c2(0.0, 0.0);
+                    }
+#pragma unroll
+                    for (int aa = 0; aa < TM; ++aa)
+#pragma unroll
+                        for (int bb = 0; bb < TM; ++bb) acc[aa][bb] = cfma(acc[aa][bb], xv[aa], tv[bb]);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int aa = 0; aa < TM; ++aa)
+#pragma unroll
+                    for (int bb = 0; bb < TM; ++bb) {
+                        const int i = tr + 16 * aa, j = tc + 16 * bb;
+                        if (i < n && j < n && i >= j) {
+                            double2 c = acc[aa][bb];
+                            if (i == j) c.y = 0.0;
+                            B[i + (size_t)j * ld] = c;
+                            B[j + (size_t)i * ld] = cconj(c);
+                        }
+                    }
+                __syncthreads();
+            }
+        }
+
+        if (!code && a.stage == 2) {
+            for (int j = tr; j < n; j += 16)
+                for (int i = tc; i < n; i += 16) Ub[i + (size_t)j * n] = B[i + (size_t)j * ld];
+            if (tid == 0) a.info[b] = 0;
+            continue;
+        }
+
+        if (!code) {
+            // ---- a5a: Householder tridiagonalisation of C (lower). Reflector k:
+            // I - tau_k v v^H on rows k+1.., v[k+1] = 1, v[k+2..] kept in A's
+            // strict upper triangle (row k), tau_k in v.tau.
+            for (int k = 0; k < n - 1; ++k) {
+                const double2* bk = B + (size_t)k * ld;
+                if (warp == 0) {
+                    double ss = 0.0;
+                    for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = bk[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                    ss = warp_sum(ss);
+                    const double2 alpha = bk[k + 1];
+                    double2 taui, scal = c2(0.0, 0.0);
+                    double beta;
+                    if (ss == 0.0 && alpha.y == 0.0) {
+                        taui = c2(0.0, 0.0);
+                        beta = alpha.x;
+                    } else {
+                        beta = -copysign(sqrt(fma(alpha.x, alpha.x, fma(alpha.y, alpha.y, ss))), alpha.x);
+                        const double rb = fast_rcp(beta);
+                        taui = c2((beta - alpha.x) * rb, -alpha.y * rb);
+                        const double2 z = c2(alpha.x - beta, alpha.y);
+                        const double inv = fast_rcp(fma(z.x, z.x, z.y * z.y));
+                        scal = c2(z.x * inv, -z.y * inv);
+                    }
+                    for (int i = k + 2 + lane; i < n; i += 32) {
+                        const double2 vi = cmul(bk[i], scal);
+                        v.vb[i] = vi;
+                        A[k + (size_t)i * ld] = vi;
+                    }
+                    if (lane == 0) {
+                        v.vb[k + 1] = c2(1.0, 0.0);
+                        v.tau[k] = taui;
+                        v.d[k] = bk[k].x;
+                        v.e[k] = beta;
+                    }
+                }
+                __syncthreads();
+                const double2 taui = v.tau[k];
+                if (taui.x == 0.0 && taui.y == 0.0) continue;
+                // p = tau A22 v: four lanes per row; per-warp partial of p^H v
+                {
+                    double2 dotp = c2(0.0, 0.0);
+                    for (int i = k + 1 + g; i < n; i += kNG) {
+                        double2 acc = c2(0.0, 0.0);
+                        for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], v.vb[j]);
+                        acc = group_sum2<kG>(gmask, acc);
+                        const double2 pi = cmul(taui, acc);
+                        if (q == 0) { v.pb[i] = pi; dotp = cfmac(dotp, pi, v.vb[i]); }
+                    }
+                    dotp = warp_sum2(dotp);
+                    if (lane == 0) v.wred[warp] = dotp;
+                }
+                __syncthreads();
+                // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v)
+                {
+                    double2 dot = c2(0.0, 0.0);
+#pragma unroll
+                    for (int w = 0; w < kNT / 32; ++w) dot = cadd(dot, v.wred[w]);
+                    const double2 alpha2 = cscale(cmul(taui, dot), -0.5);
+                    double2 vi[TM], wi[TM], vj[TM], wj[TM];
+#pragma unroll
+                    for (int t = 0; t < TM; ++t) {
+                        const int i = k + 1 + tr + 16 * t, j = k + 1 + tc + 16 * t;
+                        vi[t] = (i < n) ? v.vb[i] : c2(0.0, 0.0);
+                        wi[t] = (i < n) ? cfma(v.pb[i], alpha2, vi[t]) : c2(0.0, 0.0);
+                        vj[t] = (j < n) ? v.vb[j] : c2(0.0, 0.0);
+                        wj[t] = (j < n) ? cfma(v.pb[j], alpha2, vj[t]) : c2(0.0, 0.0);
+                    }
+#pragma unroll
+                    for (int bb = 0; bb < TM; ++bb) {
+                        const int j = k + 1 + tc + 16 * bb;
+                        if (j >= n) break;
+                        double2* bj = B + (size_t)j * ld;
+#pragma unroll
+                        for (int aa = 0; aa < TM; ++aa) {
+                            const int i = k + 1 + tr + 16 * aa;
+                            if (i >= n) break;
+                            double2 x = bj[i];
+                            x = cfms_bc(x, vi[aa], wj[bb]);
+                            x = cfms_bc(x, wi[aa], vj[bb]);
+                            bj[i] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            if (tid == 0) v.d[n - 1] = B[(n - 1) + (size_t)(n - 1) * ld].x;
+            __syncthreads();
+            // ---- a5b: divide and conquer; Z (real) and its workspace in B
+            DCShared dc;
+            dc.Z = reinterpret_cast<double*>(B); dc.ldz = ld;
+            dc.U = dc.Z + (size_t)n * ld;        dc.ldu = ld;
+            dc.d = v.d; dc.e = v.e;
+            dc.w = v.dcd; dc.z = dc.w + n; dc.dl = dc.z + n; dc.zz = dc.dl + n; dc.zh = dc.zz + n;
+            dc.rt = dc.zh + n; dc.rho = dc.rt + n; dc.scal = dc.rho + n;
+            dc.org = v.dci; dc.nd = dc.org + n; dc.perm = dc.nd + n; dc.kcnt = dc.perm + n;
+            tridiag_dc<kNT, NMAX>(n, dc);
+            if (tid == 0) {
+                bool bad = false;
+                for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
+                v.ctl[4] = bad ? n : 0;
+            }
+            __syncthreads();
+            if (v.ctl[4]) code = v.ctl[4];
+        }
+
+        if (code) {
+            const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+            for (size_t idx = tid; idx < nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
+            if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
+            if (tid == 0) a.info[b] = code;
+            continue;
+        }
+
+        // ---- ascending rank of each eigenvalue
+        for (int j = tid; j < n; j += kNT) {
+            const double dj = order_key(v.dcd[j]);
+            int r = 0;
+            for (int k2 = 0; k2 < n; ++k2) {
+                const double dk = order_key(v.dcd[k2]);
+                r += (dk < dj) || (dk == dj && k2 < j);
+            }
+            v.rank[j] = r;
+            Wb[r] = v.dcd[j];
+        }
+        // ---- a5c: V = Q Z, one column per four-lane group, in registers.
+        // Reflectors are applied in blocks of 16 (k from 16c+15 down to 16c);
+        // rows below 16c are untouched by a block, so the loops over a lane's
+        // rows start at the block (compile-time bounds), predicated only
+        // inside the diagonal block.
+        {
+            double2 x[R];
+            const double* Z = reinterpret_cast<const double*>(B);
+            const int j = g;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int i = q + kG * t;
+                x[t] = c2((j < n && i < n) ? Z[i + (size_t)j * ld] : 0.0, 0.0);
+            }
+            __syncthreads();   // B is free from here on
+            if (j < n) {
+#pragma unroll
+                for (int c = NMAX / 16 - 1; c >= 0; --c) {
+                    const int khi = min(16 * c + 15, n - 2);
+                    for (int k = khi; k >= 16 * c; --k) {
+                        const double2 tk = v.tau[k];
+                        if (tk.x == 0.0 && tk.y == 0.0) continue;
+                        const double2* vk = A + k;   // v_k[i] = vk[i*ld] (i >= k+2), v_k[k+1] = 1
+                        double2 s = c2(0.0, 0.0);
+#pragma unroll
+                        for (int t = 4 * c; t < R; ++t) {
+                            const int i = q + kG * t;
+                            if (i > k && i < n) {
+                                const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                                s = cfmac(s, vi, x[t]);
+                            }
+                        }
+                        s = group_sum2<kG>(gmask, s);
+                        const double2 ts = cmul(tk, s);
+#pragma unroll
+                        for (int t = 4 * c; t < R; ++t) {
+                            const int i = q + kG * t;
+                            if (i > k && i < n) {
+                                const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
+                                x[t] = cfms(x[t], ts, vi);
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    const int i = q + kG * t;
+                    if (i < n) B[i + (size_t)j * ld] = x[t];
+                }
+            }
+        }
+        __syncthreads();
+        if (a.stage == 3) {
+            for (int jj = tr; jj < n; jj += 16) {
+                double2* uo = Ub + (size_t)v.rank[jj] * n;
+                for (int i = tc; i < n; i += 16) uo[i] = B[i + (size_t)jj * ld];
+            }
+            if (tid == 0) a.info[b] = 0;
+            continue;
+        }
+        // ---- a6: U = X^H V, U(i, j) = sum_{k >= i} conj(X(k, i)) V(k, j)
+        {
+            double2 acc[TM][TM];
+            tile_zero<TM>(acc);
+            for (int k = tr; k < n; ++k) {
+                double2 xv[TM], vv[TM];
+#pragma unroll
+                for (int t = 0; t < TM; ++t) {
+                    const int i = tr + 16 * t, j = tc + 16 * t;
+                    xv[t] = (i < n && k >= i) ? cconj(A[k + (size_t)i * ld]) : c2(0.0, 0.0);
+                    vv[t] = (j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int aa = 0; aa < TM; ++aa)
+#pragma unroll
+                    for (int bb = 0; bb < TM; ++bb) acc[aa][bb] = cfma(acc[aa][bb], xv[aa], vv[bb]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int aa = 0; aa < TM; ++aa)
+#pragma unroll
+                for (int bb = 0; bb < TM; ++bb) {
+                    const int i = tr + 16 * aa, j = tc + 16 * bb;
+                    if (i < n && j < n) B[i + (size_t)j * ld] = acc[aa][bb];
+                }
+            __syncthreads();
+        }
+        // ---- a7: store U, column j to position rank[j]
+        for (int jj = tr; jj < n; jj += 16) {
+            double2* uo = Ub + (size_t)v.rank[jj] * n;
+            for (int i = tc; i < n; i += 16) uo[i] = B[i + (size_t)jj * ld];
+        }
+        if (tid == 0) a.info[b] = 0;
+    }
+}
+
+}  // namespace
+
+size_t cta_smem_bytes(int n) { return (size_t)2 * n * (n | 1) * 16 + cta_vec_bytes(n); }
+
+int cta_nmax_for(int n) { return n <= 16 ? 16 : n <= 32 ? 32 : n <= 48 ? 48 : 64; }
+
+using CtaKernelFn = void (*)(CtaArgs);
+static CtaKernelFn cta_kernel_for(int nmax) {
+    switch (nmax) {
+        case 16: return geneig_cta_kernel<16>;
+        case 32: return geneig_cta_kernel<32>;
+        case 48: return geneig_cta_kernel<48>;
+        default: return geneig_cta_kernel<64>;
+    }
+}
+
+cudaError_t cta_set_attributes(int nmax, size_t smem) {
+    return cudaFuncSetAttribute(cta_kernel_for(nmax), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
+                       int* info, long long batch, cudaStream_t stream) {
+    CtaArgs a;
+    a.H = static_cast<const double2*>(H);
+    a.S = static_cast<const double2*>(S);
+    a.W = W;
+    a.U = static_cast<double2*>(U);
+    a.info = info;
+    a.batch = batch;
+    a.n = n;
+    a.ld = n | 1;
+    a.stage = stage;
+    const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
+    cta_kernel_for(nmax)<<<(unsigned)grid, kNT, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace sgeig

@@ -15,9 +15,18 @@ int smem_cta_max_n();
 
 // How one solve is laid out on the device.
 enum class Regime : int {
-    SmemCta = 0,   // S->L and H->C->V->U resident in one CTA's shared memory
-    L2Slot  = 1,   // both matrices in a per-CTA global-memory slot (L2 resident)
+    SmemCta  = 0,  // N <= 64: both matrices in one CTA's shared memory, GEMM-tiled kernel
+    SmemWide = 1,  // N <= 83: both matrices in shared memory, column-group kernel
+    L2Slot   = 2,  // both matrices in a per-CTA global-memory slot (L2 resident)
 };
+
+// Shared-memory kernel for N <= 64 (geneig_cta.cu).
+constexpr int kCtaMaxN = 64;
+size_t cta_smem_bytes(int n);
+int cta_nmax_for(int n);
+cudaError_t cta_set_attributes(int nmax, size_t smem);
+cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
+                       int* info, long long batch, cudaStream_t stream);
 
 struct PlainPlan {
     int    n        = 0;

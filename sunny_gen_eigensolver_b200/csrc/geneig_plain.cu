@@ -462,17 +462,9 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
 
 int g_smem_optin = -1;
 
-// Register-array bound of the shared-memory regime for size n.
-int nmax_for(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : 96); }
-
 using KernelFn = void (*)(PlainArgs);
-KernelFn kernel_for(Regime r, int nmax) {
-    if (r == Regime::L2Slot) return geneig_plain_kernel<true, 0>;
-    switch (nmax) {
-        case 32: return geneig_plain_kernel<false, 32>;
-        case 64: return geneig_plain_kernel<false, 64>;
-        default: return geneig_plain_kernel<false, 96>;
-    }
+KernelFn kernel_for(Regime r) {
+    return (r == Regime::L2Slot) ? geneig_plain_kernel<true, 0> : geneig_plain_kernel<false, 96>;
 }
 
 }  // namespace
@@ -504,18 +496,25 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
     p.n = n;
     p.ld = n | 1;
     p.threads = kNT;
-    const size_t smem_cta = (size_t)2 * n * p.ld * 16 + vec_area_bytes(n);
-    if (smem_cta <= (size_t)optin && n <= 96) {
+    const size_t smem_wide = (size_t)2 * n * p.ld * 16 + vec_area_bytes(n);
+    if (n <= kCtaMaxN && cta_smem_bytes(n) <= (size_t)optin) {
         p.regime = Regime::SmemCta;
-        p.smem = smem_cta;
-        p.nmax = nmax_for(n);
+        p.smem = cta_smem_bytes(n);
+        p.nmax = cta_nmax_for(n);
+        e = cta_set_attributes(p.nmax, p.smem);
     } else {
-        p.regime = Regime::L2Slot;
-        p.smem = vec_area_bytes(n);
-        p.slots = 2 * sms;
-        p.scratch_bytes = (size_t)p.slots * 2 * n * p.ld * 16;
+        if (smem_wide <= (size_t)optin && n <= 96) {
+            p.regime = Regime::SmemWide;
+            p.smem = smem_wide;
+            p.nmax = 96;
+        } else {
+            p.regime = Regime::L2Slot;
+            p.smem = vec_area_bytes(n);
+            p.slots = 2 * sms;
+            p.scratch_bytes = (size_t)p.slots * 2 * n * p.ld * 16;
+        }
+        e = cudaFuncSetAttribute(kernel_for(p.regime), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     }
-    e = cudaFuncSetAttribute(kernel_for(p.regime, p.nmax), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
     *plan = p;
     return true;
@@ -535,9 +534,11 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const 
     a.n = plan.n;
     a.ld = plan.ld;
     a.stage = stage;
+    if (plan.regime == Regime::SmemCta)
+        return cta_launch(plan.n, plan.nmax, plan.smem, stage, H, S, W, U, info, batch, stream);
     long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
     if (plan.regime == Regime::L2Slot && grid > plan.slots) grid = plan.slots;
-    kernel_for(plan.regime, plan.nmax)<<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
+    kernel_for(plan.regime)<<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
     return cudaGetLastError();
 }
 
