@@ -136,26 +136,22 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                 }
                 if (tid == 0) v.rdg[c] = rprev;
             }
+            // trailing update: group g takes row i = k+1+g (active rows map to the
+            // low groups, so finished rows leave whole warps idle); its four lanes
+            // take columns j = k+1+q, k+5+q, ... <= i
             const double r2 = r * r;
             const double2* ak = A + (size_t)k * ld;
-            double2 li[TM], lj[TM];
-#pragma unroll
-            for (int t = 0; t < TM; ++t) {
-                const int i = k + 1 + tr + 16 * t, j = k + 1 + tc + 16 * t;
-                li[t] = (i < n) ? ak[i] : c2(0.0, 0.0);
-                lj[t] = (j < n) ? cscale(cconj(ak[j]), r2) : c2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int bb = 0; bb < TM; ++bb) {
-                const int j = k + 1 + tc + 16 * bb;
-                if (j >= n) break;
-                double2* aj = A + (size_t)j * ld;
-#pragma unroll
-                for (int aa = 0; aa < TM; ++aa) {
-                    const int i = k + 1 + tr + 16 * aa;
-                    if (i >= n) break;
-                    if (i >= j) aj[i] = cfms(aj[i], li[aa], lj[bb]);
+            const int i = k + 1 + g;
+            if (i < n) {
+                const double2 lik = cscale(ak[i], r2);
+                int j = k + 1 + q;
+                for (; j + 4 <= i; j += 8) {
+                    const double2 x0 = A[i + (size_t)j * ld], x1 = A[i + (size_t)(j + 4) * ld];
+                    const double2 l0 = ak[j], l1 = ak[j + 4];
+                    A[i + (size_t)j * ld] = cfms_bc(x0, lik, l0);
+                    A[i + (size_t)(j + 4) * ld] = cfms_bc(x1, lik, l1);
                 }
+                if (j <= i) A[i + (size_t)j * ld] = cfms_bc(A[i + (size_t)j * ld], lik, ak[j]);
             }
             rprev = r;
         }
@@ -179,26 +175,34 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         }
 
         if (!code) {
-            // ---- L^-1 in place. Row k is finalised (X(k, j) = acc(k, j)/L_kk)
-            // by its own group, then every later row i subtracts
-            // L(i, k) X(k, :). acc(i, j) lives in the slot of L(i, j), whose
-            // last use is step j; at step k the slot (i, k) is overwritten with
-            // -L(i, k) X(k, k) after all four lanes of row i have read L(i, k).
+            // ---- X = L^-1 in place, right-looking over rows. At step k row k
+            // is finalised, X(k, j) = acc(k, j) / L_kk (group 0 did row k's last
+            // update at step k-1, with the same lane per column), then group g
+            // takes row i = k+1+g and subtracts L(i, k) X(k, :). acc(i, j) lives
+            // in the slot of L(i, j), whose last use is step j; at step k slot
+            // (i, k) receives -L(i, k) X(k, k) after all four lanes have read L(i, k).
             for (int k = 0; k < n; ++k) {
-                if (g == k % kNG) {   // finalise row k (row i is always handled by group i % 64)
+                if (g == 0) {
                     const double rk = v.rdg[k];
                     for (int j = q; j < k; j += kG) A[k + (size_t)j * ld] = cscale(A[k + (size_t)j * ld], rk);
                     if (q == 0) A[k + (size_t)k * ld] = c2(rk, 0.0);
                 }
                 __syncthreads();
-                for (int i = g; i < n; i += kNG) {
-                    if (i <= k) continue;
+                const int i = k + 1 + g;
+                if (i < n) {
                     const double2 lik = A[i + (size_t)k * ld];
                     __syncwarp(gmask);
-                    for (int j = q; j <= k; j += kG) {
+                    int j = q;
+                    for (; j + 4 < k; j += 8) {
+                        const double2 x0 = A[k + (size_t)j * ld], x1 = A[k + (size_t)(j + 4) * ld];
+                        const double2 a0 = A[i + (size_t)j * ld], a1 = A[i + (size_t)(j + 4) * ld];
+                        A[i + (size_t)j * ld] = cfms(a0, lik, x0);
+                        A[i + (size_t)(j + 4) * ld] = cfms(a1, lik, x1);
+                    }
+                    for (; j <= k; j += kG) {
                         const double2 xkj = A[k + (size_t)j * ld];
-                        double2* p = A + i + (size_t)j * ld;
-                        *p = (j == k) ? cscale(cmul(lik, xkj), -1.0) : cfms(*p, lik, xkj);
+                        A[i + (size_t)j * ld] = (j == k) ? cscale(cmul(lik, xkj), -1.0)
+                                                         : cfms(A[i + (size_t)j * ld], lik, xkj);
                     }
                 }
             }
@@ -333,34 +337,30 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                     if (lane == 0) v.wred[warp] = dotp;
                 }
                 __syncthreads();
-                // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v)
+                // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v);
+                // group g takes row i = k+1+g, its lanes columns j = k+1+q step 4
                 {
                     double2 dot = c2(0.0, 0.0);
 #pragma unroll
                     for (int w = 0; w < kNT / 32; ++w) dot = cadd(dot, v.wred[w]);
                     const double2 alpha2 = cscale(cmul(taui, dot), -0.5);
-                    double2 vi[TM], wi[TM], vj[TM], wj[TM];
-#pragma unroll
-                    for (int t = 0; t < TM; ++t) {
-                        const int i = k + 1 + tr + 16 * t, j = k + 1 + tc + 16 * t;
-                        vi[t] = (i < n) ? v.vb[i] : c2(0.0, 0.0);
-                        wi[t] = (i < n) ? cfma(v.pb[i], alpha2, vi[t]) : c2(0.0, 0.0);
-                        vj[t] = (j < n) ? v.vb[j] : c2(0.0, 0.0);
-                        wj[t] = (j < n) ? cfma(v.pb[j], alpha2, vj[t]) : c2(0.0, 0.0);
-                    }
-#pragma unroll
-                    for (int bb = 0; bb < TM; ++bb) {
-                        const int j = k + 1 + tc + 16 * bb;
-                        if (j >= n) break;
-                        double2* bj = B + (size_t)j * ld;
-#pragma unroll
-                        for (int aa = 0; aa < TM; ++aa) {
-                            const int i = k + 1 + tr + 16 * aa;
-                            if (i >= n) break;
-                            double2 x = bj[i];
-                            x = cfms_bc(x, vi[aa], wj[bb]);
-                            x = cfms_bc(x, wi[aa], vj[bb]);
-                            bj[i] = x;
+                    const int i = k + 1 + g;
+                    if (i < n) {
+                        const double2 vi = v.vb[i];
+                        const double2 wi = cfma(v.pb[i], alpha2, vi);
+                        double2* bi = B + i;
+                        int j = k + 1 + q;
+                        for (; j + 4 < n; j += 8) {
+                            const double2 x0 = bi[(size_t)j * ld], x1 = bi[(size_t)(j + 4) * ld];
+                            const double2 v0 = v.vb[j], v1 = v.vb[j + 4];
+                            const double2 w0 = cfma(v.pb[j], alpha2, v0), w1 = cfma(v.pb[j + 4], alpha2, v1);
+                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(x0, vi, w0), wi, v0);
+                            bi[(size_t)(j + 4) * ld] = cfms_bc(cfms_bc(x1, vi, w1), wi, v1);
+                        }
+                        if (j < n) {
+                            const double2 v0 = v.vb[j];
+                            const double2 w0 = cfma(v.pb[j], alpha2, v0);
+                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(bi[(size_t)j * ld], vi, w0), wi, v0);
                         }
                     }
                 }
@@ -428,16 +428,16 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                         const double2 tk = v.tau[k];
                         if (tk.x == 0.0 && tk.y == 0.0) continue;
                         const double2* vk = A + k;   // v_k[i] = vk[i*ld] (i >= k+2), v_k[k+1] = 1
-                        double2 s = c2(0.0, 0.0);
+                        double2 s0 = c2(0.0, 0.0), s1 = c2(0.0, 0.0);
 #pragma unroll
                         for (int t = 4 * c; t < R; ++t) {
                             const int i = q + kG * t;
                             if (i > k && i < n) {
                                 const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
-                                s = cfmac(s, vi, x[t]);
+                                if (t & 1) s1 = cfmac(s1, vi, x[t]); else s0 = cfmac(s0, vi, x[t]);
                             }
                         }
-                        s = group_sum2<kG>(gmask, s);
+                        double2 s = group_sum2<kG>(gmask, cadd(s0, s1));
                         const double2 ts = cmul(tk, s);
 #pragma unroll
                         for (int t = 4 * c; t < R; ++t) {

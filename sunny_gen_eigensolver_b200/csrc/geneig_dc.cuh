@@ -47,32 +47,65 @@ struct DCShared {
     double* scal;           // [0] = scale applied to T
 };
 
+// Largest power of two strictly below x (x >= 2).
+__host__ __device__ constexpr int top_bit(int x) { return (x & (x - 1)) ? top_bit(x & (x - 1)) : x; }
+__host__ __device__ constexpr int pow2_below(int x) { return (x & (x - 1)) ? top_bit(x) : x / 2; }
+static_assert(pow2_below(48) == 32 && pow2_below(64) == 32 && pow2_below(32) == 16 && pow2_below(16) == 8, "pow2_below");
+
 // Number of doubles / ints of scratch DCShared needs for size n (excluding Z, U).
 __host__ __device__ inline int dc_vec_doubles(int n) { return 8 * n + 2; }
 __host__ __device__ inline int dc_vec_ints(int n) { return 4 * n; }
 
+// Sum over the P consecutive lanes that share one root (P = 1, 2 or 4); on
+// the host (P = 1) it is the identity. Every lane ends with the same value
+// (the butterfly adds the same pairs in the same order up to commutation).
+template <int P>
+__host__ __device__ __forceinline__ double lanes_sum(double v, unsigned mask) {
+#ifdef __CUDA_ARCH__
+    if (P >= 2) v += __shfl_xor_sync(mask, v, 1);
+    if (P >= 4) v += __shfl_xor_sync(mask, v, 2);
+#else
+    (void)mask;
+#endif
+    return v;
+}
+template <int P>
+__host__ __device__ __forceinline__ double lanes_prod(double v, unsigned mask) {
+#ifdef __CUDA_ARCH__
+    if (P >= 2) v *= __shfl_xor_sync(mask, v, 1);
+    if (P >= 4) v *= __shfl_xor_sync(mask, v, 2);
+#else
+    (void)mask;
+#endif
+    return v;
+}
+
 // Root i (0-based) of 1 + rho sum_j zz_j^2 / (dl_j - x) = 0 with dl ascending,
-// rho > 0. Returns the offset tau of the root from pole `org`; the return
-// value is the number of iterations taken.
-__host__ __device__ inline int secular_root(int i, int K, const double* dl, const double* zz, double rho,
-                                            double& tau_out, int& org_out) {
+// rho > 0, computed by P lanes together (lane qq sums the terms j = qq mod P).
+// Returns the offset tau of the root from pole `org`; the return value is the
+// number of iterations taken.
+template <int P>
+__host__ __device__ inline int secular_root_p(int i, int K, const double* dl, const double* zz, double rho,
+                                              int qq, unsigned mask, double& tau_out, int& org_out) {
     if (K == 1) { org_out = 0; tau_out = rho * zz[0] * zz[0]; return 0; }
     int o;
     double lo, hi, tau;
     if (i < K - 1) {
         const double gap = dl[i + 1] - dl[i];
         const double mid = 0.5 * gap;
-        double g = 1.0;
-        for (int j = 0; j < K; ++j) {
+        double gs = 0.0;
+#pragma unroll 4
+        for (int j = qq; j < K; j += P) {
             const double del = (dl[j] - dl[i]) - mid;
-            g += rho * zz[j] * (zz[j] * fast_rcp(del));
+            gs = fma(rho * zz[j], zz[j] * fast_rcp(del), gs);
         }
+        const double g = 1.0 + lanes_sum<P>(gs, mask);
         if (g >= 0.0) { o = i;     lo = 0.0;  hi = mid; tau = mid; }
         else          { o = i + 1; lo = -mid; hi = 0.0; tau = -mid; }
     } else {
-        double s = 0.0;
-        for (int j = 0; j < K; ++j) s += zz[j] * zz[j];
-        o = K - 1; lo = 0.0; hi = rho * s; tau = hi;
+        double ss = 0.0;
+        for (int j = qq; j < K; j += P) ss += zz[j] * zz[j];
+        o = K - 1; lo = 0.0; hi = rho * lanes_sum<P>(ss, mask); tau = hi;
     }
     const double dlo = dl[o];
     const double p = dl[i] - dlo;
@@ -80,15 +113,24 @@ __host__ __device__ inline int secular_root(int i, int K, const double* dl, cons
     int it = 0;
     for (; it < 80; ++it) {
         double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0, erra = 0.0;
-        for (int j = 0; j < K; ++j) {
+#pragma unroll 4
+        for (int j = qq; j < K; j += P) {
             const double del = (dl[j] - dlo) - tau;
             const double t = zz[j] * fast_rcp(del);
             const double term = rho * zz[j] * t;
             const double dterm = rho * t * t;
-            if (j <= i) { psi += term; dpsi += dterm; }
-            else        { phi += term; dphi += dterm; }
+            const bool left = j <= i;       // poles left of the root go to psi
+            psi += left ? term : 0.0;
+            dpsi += left ? dterm : 0.0;
+            phi += left ? 0.0 : term;
+            dphi += left ? 0.0 : dterm;
             erra += fabs(term);
         }
+        psi = lanes_sum<P>(psi, mask);
+        dpsi = lanes_sum<P>(dpsi, mask);
+        phi = lanes_sum<P>(phi, mask);
+        dphi = lanes_sum<P>(dphi, mask);
+        erra = lanes_sum<P>(erra, mask);
         const double g = 1.0 + psi + phi;
         const double err = kEps * (2.0 + 8.0 * erra + 3.0 * fabs(tau) * (dpsi + dphi));
         if (fabs(g) <= err) break;
@@ -112,8 +154,8 @@ __host__ __device__ inline int secular_root(int i, int K, const double* dl, cons
             } else {
                 double disc = B * B - 4.0 * c * C;
                 if (disc < 0.0) disc = 0.0;
-                const double qq = -0.5 * (B + copysign(sqrt(disc), B));
-                const double x1 = qq / c, x2 = (qq != 0.0) ? C / qq : x1;
+                const double qq2 = -0.5 * (B + copysign(sqrt(disc), B));
+                const double x1 = qq2 / c, x2 = (qq2 != 0.0) ? C / qq2 : x1;
                 tn = (x1 > lo && x1 < hi) ? x1 : x2;
             }
         } else {
@@ -135,6 +177,12 @@ __host__ __device__ inline int secular_root(int i, int K, const double* dl, cons
     tau_out = tau;
     org_out = o;
     return it;
+}
+
+// Single-lane form (host tests and callers without lane groups).
+__host__ __device__ inline int secular_root(int i, int K, const double* dl, const double* zz, double rho,
+                                            double& tau_out, int& org_out) {
+    return secular_root_p<1>(i, K, dl, zz, rho, 0, 0u, tau_out, org_out);
 }
 
 // All NT threads of the CTA call this. n >= 1. On return Z, w hold the
@@ -267,37 +315,47 @@ __device__ void tridiag_dc(int n, DCShared s) {
             }
         }
         __syncthreads();
-        // ---- phase B: secular roots, one thread per root
-        for (int pidx = tid; pidx < n; pidx += NT) {
+        // ---- phase B: secular roots, four lanes per root (root slot = tid / 4)
+        for (int p0 = 0; p0 < 4 * n; p0 += NT) {
+            const int pidx = (p0 + tid) >> 2, qq = tid & 3;
+            const unsigned qmask = 0xFu << (lane & ~3);
+            if (pidx >= n) continue;
             const int a = pidx - pidx % span;
             if (a + half >= n) continue;
             const int i = pidx - a, K = s.kcnt[a];
             if (i >= K) continue;
             double t; int o;
-            secular_root(i, K, s.dl + a, s.zz + a, s.rho[a], t, o);
-            s.rt[pidx] = t;
-            s.org[pidx] = o;
+            secular_root_p<4>(i, K, s.dl + a, s.zz + a, s.rho[a], qq, qmask, t, o);
+            if (qq == 0) { s.rt[pidx] = t; s.org[pidx] = o; }
         }
         __syncthreads();
-        // ---- phase C: Loewner z-hat
-        for (int pidx = tid; pidx < n; pidx += NT) {
+        // ---- phase C: Loewner z-hat, four lanes per root
+        for (int p0 = 0; p0 < 4 * n; p0 += NT) {
+            const int pidx = (p0 + tid) >> 2, qq = tid & 3;
+            const unsigned qmask = 0xFu << (lane & ~3);
+            if (pidx >= n) continue;
             const int a = pidx - pidx % span;
             if (a + half >= n) continue;
             const int i = pidx - a, K = s.kcnt[a];
             if (i >= K) continue;
             const double* dl = s.dl + a;
             const double dli = dl[i];
-            double W = (dli - dl[s.org[a + i]]) - s.rt[a + i];
-            for (int j = 0; j < K; ++j) {
+            double W = (qq == 0) ? (dli - dl[s.org[a + i]]) - s.rt[a + i] : 1.0;
+            for (int j = qq; j < K; j += 4) {
                 if (j == i) continue;
                 const double del = (dli - dl[s.org[a + j]]) - s.rt[a + j];
                 W *= del * fast_rcp(dli - dl[j]);
             }
-            s.zh[pidx] = copysign(sqrt(fmax(-W, 0.0)), s.zz[pidx]);
+            W = lanes_prod<4>(W, qmask);
+            if (qq == 0) s.zh[pidx] = copysign(sqrt(fmax(-W, 0.0)), s.zz[pidx]);
         }
         __syncthreads();
-        // ---- phase D: eigenvector columns of the rank-one problem, new eigenvalues
-        for (int pidx = tid; pidx < n; pidx += NT) {
+        // ---- phase D: eigenvector columns of the rank-one problem (four lanes
+        // per column), new eigenvalues
+        for (int p0 = 0; p0 < 4 * n; p0 += NT) {
+            const int pidx = (p0 + tid) >> 2, qq = tid & 3;
+            const unsigned qmask = 0xFu << (lane & ~3);
+            if (pidx >= n) continue;
             const int a = pidx - pidx % span;
             if (a + half >= n) continue;
             const int j = pidx - a, K = s.kcnt[a];
@@ -306,36 +364,83 @@ __device__ void tridiag_dc(int n, DCShared s) {
             const double base = dl[s.org[a + j]], tj = s.rt[a + j];
             double* ucol = s.U + a + (size_t)(a + j) * s.ldu;
             double nrm = 0.0;
-            for (int l = 0; l < K; ++l) {
+            for (int l = qq; l < K; l += 4) {
                 const double v = s.zh[a + l] * fast_rcp((dl[l] - base) - tj);
                 ucol[l] = v;
                 nrm = fma(v, v, nrm);
             }
-            const double inv = rsqrt(nrm);
-            for (int l = 0; l < K; ++l) ucol[l] *= inv;
-            s.w[s.nd[a + j]] = base + tj;
+            const double inv = rsqrt(lanes_sum<4>(nrm, qmask));
+            for (int l = qq; l < K; l += 4) ucol[l] *= inv;
+            if (qq == 0) s.w[s.nd[a + j]] = base + tj;
         }
         __syncthreads();
-        // ---- phase E: Z(:, nd) <- Z(:, nd) * U, row-parallel (4 threads per row)
-        for (int p0 = 0; p0 < 4 * n; p0 += NT) {
-            const int pidx = p0 + tid;
-            const int r = pidx >> 2, part = pidx & 3;
-            const int a = (r < n) ? r - r % span : n;
-            const bool active = r < n && a + half < n && s.kcnt[a] > 0;
-            const int K = active ? s.kcnt[a] : 0;
-            double qrow[NMAX];
+        // ---- phase E: Z(:, nd) <- Z(:, nd) * U.
+        if (span >= n) {
+            // one merge over [0, n): 16 x 16 threads with register tiles
+            // (rows tr + 16 x, output columns tc + 16 y); all reads finish
+            // before the barrier, then the tiles are written back.
+            constexpr int TM = NMAX / 16;
+            const int tr = tid >> 4, tc = tid & 15;
+            const int K = s.kcnt[0];
+            double acc[TM][TM];
 #pragma unroll
-            for (int l = 0; l < NMAX; ++l) qrow[l] = (l < K) ? s.Z[r + s.nd[a + l] * s.ldz] : 0.0;
-            __syncwarp();
-            for (int j = part; j < K; j += 4) {
-                const double* ucol = s.U + a + (size_t)(a + j) * s.ldu;
-                double acc = 0.0;
+            for (int x = 0; x < TM; ++x)
 #pragma unroll
-                for (int l = 0; l < NMAX; ++l) {
-                    if (l >= K) break;
-                    acc = fma(qrow[l], ucol[l], acc);
+                for (int y = 0; y < TM; ++y) acc[x][y] = 0.0;
+            if (K > 0) {
+                for (int l = 0; l < K; ++l) {
+                    const double* zc = s.Z + (size_t)s.nd[l] * s.ldz;
+                    const double* ur = s.U + l;
+                    double zr[TM], uc[TM];
+#pragma unroll
+                    for (int t = 0; t < TM; ++t) {
+                        const int r = tr + 16 * t, j = tc + 16 * t;
+                        zr[t] = (r < n) ? zc[r] : 0.0;
+                        uc[t] = (j < K) ? ur[(size_t)j * s.ldu] : 0.0;
+                    }
+#pragma unroll
+                    for (int x = 0; x < TM; ++x)
+#pragma unroll
+                        for (int y = 0; y < TM; ++y) acc[x][y] = fma(zr[x], uc[y], acc[x][y]);
                 }
-                s.Z[r + s.nd[a + j] * s.ldz] = acc;
+            }
+            __syncthreads();
+            if (K > 0) {
+#pragma unroll
+                for (int x = 0; x < TM; ++x)
+#pragma unroll
+                    for (int y = 0; y < TM; ++y) {
+                        const int r = tr + 16 * x, j = tc + 16 * y;
+                        if (r < n && j < K) s.Z[r + (size_t)s.nd[j] * s.ldz] = acc[x][y];
+                    }
+            }
+        } else {
+            // several merges, each of at most `span` columns, span being at most
+            // the largest power of two below NMAX: four lanes per row, lane q
+            // accumulating output columns j = q + 4u in registers
+            constexpr int UMAX = pow2_below(NMAX) / 4;
+            for (int p0 = 0; p0 < 4 * n; p0 += NT) {
+                const int pidx = p0 + tid;
+                const int r = pidx >> 2, part = pidx & 3;
+                const int a = (r < n) ? r - r % span : n;
+                const bool active = r < n && a + half < n && s.kcnt[a] > 0;
+                const int K = active ? s.kcnt[a] : 0;
+                double acc[UMAX];
+#pragma unroll
+                for (int u = 0; u < UMAX; ++u) acc[u] = 0.0;
+                for (int l = 0; l < K; ++l) {
+                    const double x = s.Z[r + (size_t)s.nd[a + l] * s.ldz];
+                    const double* ur = s.U + (a + l) + (size_t)(a + part) * s.ldu;
+#pragma unroll
+                    for (int u = 0; u < UMAX; ++u)
+                        if (part + 4 * u < K) acc[u] = fma(x, ur[(size_t)(4 * u) * s.ldu], acc[u]);
+                }
+                __syncwarp();
+#pragma unroll
+                for (int u = 0; u < UMAX; ++u) {
+                    const int j = part + 4 * u;
+                    if (j < K) s.Z[r + (size_t)s.nd[a + j] * s.ldz] = acc[u];
+                }
             }
         }
         __syncthreads();
