@@ -154,6 +154,31 @@ const char* sunny_geneig_regime_name(sunny_geneig_solver_t solver);
 sunny_geneig_status_t sunny_geneig_selftest_reciprocal(uintptr_t d_x, uintptr_t d_out, int n,
                                                        uintptr_t stream);
 
+/* Allocation-free solve (no counterpart in the reference's C ABI).
+ * For callers that cannot allocate device memory: code running inside
+ * another framework's memory pool or under a no-allocation policy, hosts
+ * that forbid cudaMalloc from plugins, graph-replay setups that must not
+ * touch the allocator. Same buffers, layouts, info codes and error
+ * behaviour as sunny_geneig_launch, on the calling thread's current device,
+ * with no handle: it runs the L2-slot kernel with its per-CTA scratch taken
+ * from a fixed 32 MiB device array built into the library (held by every
+ * GPU that loads the library until the process exits), so it allocates
+ * nothing. n outside [1, 512] is rejected with INVALID_ARG. The first call
+ * on a device resolves the array's address and sets the kernel's
+ * shared-memory limit; make that first call before any stream capture.
+ * All calls share the one array: calls whose kernels overlap on the GPU
+ * (other streams, other host threads) race on it and must be serialised by
+ * the caller. */
+sunny_geneig_status_t sunny_geneig_launch_noalloc(
+    int                   n,
+    uintptr_t             d_H,
+    uintptr_t             d_S,
+    uintptr_t             d_W,
+    uintptr_t             d_U,
+    uintptr_t             d_info,
+    int                   batch_size,
+    uintptr_t             stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

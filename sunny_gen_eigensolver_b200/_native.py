@@ -28,7 +28,7 @@ EXPORTS = (
     "sunny_geneig_matrix_size", "sunny_geneig_batches_per_block", "sunny_geneig_block_dim_x",
     "sunny_geneig_shared_mem_bytes", "sunny_geneig_last_error", "sunny_geneig_path_name",
     "sunny_geneig_kernel_mode", "sunny_geneig_launch_stage", "sunny_geneig_max_matrix_size",
-    "sunny_geneig_regime_name", "sunny_geneig_selftest_reciprocal",
+    "sunny_geneig_regime_name", "sunny_geneig_selftest_reciprocal", "sunny_geneig_launch_noalloc",
 )
 
 _lib = None
@@ -73,6 +73,8 @@ def load() -> ctypes.CDLL:
     L.sunny_geneig_path_name.restype = c_char_p
     L.sunny_geneig_regime_name.argtypes = [c_void_p]
     L.sunny_geneig_regime_name.restype = c_char_p
+    L.sunny_geneig_launch_noalloc.argtypes = [c_int, c_size, c_size, c_size, c_size, c_size, c_int, c_size]
+    L.sunny_geneig_launch_noalloc.restype = c_int
     L.sunny_geneig_selftest_reciprocal.argtypes = [c_size, c_size, c_int, c_size]
     L.sunny_geneig_selftest_reciprocal.restype = c_int
     L.sunny_geneig_max_matrix_size.argtypes = []

@@ -148,6 +148,11 @@ sunny_geneig_status_t launch_impl(sunny_geneig_solver_t s, int stage, uintptr_t 
 
 }  // namespace
 
+namespace sgeig {
+void api_set_error(const std::string& msg) { set_error(msg); }
+void api_clear_error() { clear_error(); }
+}  // namespace sgeig
+
 #pragma GCC visibility push(default)
 extern "C" {
 

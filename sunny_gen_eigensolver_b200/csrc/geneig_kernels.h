@@ -50,4 +50,9 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage,
                          int* info, long long batch, void* scratch,
                          cudaStream_t stream);
 
+// Thread-local last-error text of the C ABI (defined in c_api.cpp), for
+// entry points implemented in other translation units.
+void api_set_error(const std::string& msg);
+void api_clear_error();
+
 }  // namespace sgeig

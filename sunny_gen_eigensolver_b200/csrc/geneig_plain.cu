@@ -20,9 +20,11 @@
 #include "geneig_common.cuh"
 #include "geneig_dc.cuh"
 #include "geneig_kernels.h"
+#include "sunny_geneig.h"
 
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 
 namespace sgeig {
 namespace {
@@ -542,4 +544,116 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const 
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free entry point (no counterpart in the reference).
+//
+// Callers that cannot allocate device memory -- code running inside another
+// framework's memory pool or under a strict no-allocation policy, plugins
+// whose host forbids cudaMalloc on its streams, and graph-replay setups that
+// must not touch the allocator -- get the L2-slot kernel with its per-CTA
+// scratch slots taken from the fixed array below instead of a cudaMalloc'd
+// buffer. The array is sized once (kNoAllocScratchBytes) and every GPU that
+// loads the library keeps it for the life of the process.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;   // 32 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocDevice {
+    bool ready = false;
+    void* scratch = nullptr;   // device address of g_noalloc_scratch on this device
+    int sms = 0;
+};
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+// Once per device, with that device current: resolve the array's device
+// address (the host-side symbol is only a stand-in and must never be handed
+// to a kernel) and set the kernel's shared-memory limit.
+cudaError_t noalloc_setup(int dev, NoAllocDevice** out, std::string* err) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) { *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return e; }
+        e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return e; }
+        e = cudaFuncSetAttribute(geneig_plain_kernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)vec_area_bytes(kMaxN));
+        if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return e; }
+        d.scratch = ptr;
+        d.ready = true;
+    }
+    *out = &d;
+    return cudaSuccess;
+}
+
+}  // namespace
 }  // namespace sgeig
+
+#pragma GCC visibility push(default)
+extern "C" sunny_geneig_status_t sunny_geneig_launch_noalloc(int n, uintptr_t d_H, uintptr_t d_S, uintptr_t d_W,
+                                                             uintptr_t d_U, uintptr_t d_info, int batch_size,
+                                                             uintptr_t stream) {
+    using namespace sgeig;
+    api_clear_error();
+    const size_t slot = (n >= 1) ? (size_t)2 * n * (size_t)(n | 1) * 16 : 0;
+    if (n < 1 || n > kMaxN || slot > kNoAllocScratchBytes) {
+        api_set_error("sunny_geneig_launch_noalloc: n=" + std::to_string(n) + " outside [1, " +
+                      std::to_string(kMaxN) + "] (the static scratch holds " +
+                      std::to_string(kNoAllocScratchBytes >> 20) + " MiB)");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (batch_size < 0) { api_set_error("sunny_geneig_launch_noalloc: batch_size < 0"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (batch_size == 0) return SUNNY_GENEIG_OK;
+    if (!d_H || !d_S || !d_W || !d_U || !d_info) {
+        api_set_error("sunny_geneig_launch_noalloc: NULL device buffer");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (d_H % 16 || d_S % 16 || d_U % 16 || d_W % 8 || d_info % 4) {
+        api_set_error("sunny_geneig_launch_noalloc: misaligned device buffer (H, S, U need 16 B; W 8 B; info 4 B)");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        api_set_error(std::string("sunny_geneig_launch_noalloc: no usable current device: ") + cudaGetErrorString(e));
+        return SUNNY_GENEIG_DEVICE_ERROR;
+    }
+    NoAllocDevice* d = nullptr;
+    std::string err;
+    if (noalloc_setup(dev, &d, &err) != cudaSuccess) {
+        api_set_error("sunny_geneig_launch_noalloc: " + err);
+        return SUNNY_GENEIG_DEVICE_ERROR;
+    }
+    PlainPlan p;
+    p.n = n;
+    p.ld = n | 1;
+    p.threads = kNT;
+    p.regime = Regime::L2Slot;
+    p.smem = vec_area_bytes(n);
+    const long long fit = (long long)(kNoAllocScratchBytes / slot);
+    p.slots = (int)(fit < 2LL * d->sms ? fit : 2LL * d->sms);
+    PlainArgs a;
+    a.H = reinterpret_cast<const double2*>(d_H);
+    a.S = reinterpret_cast<const double2*>(d_S);
+    a.W = reinterpret_cast<double*>(d_W);
+    a.U = reinterpret_cast<double2*>(d_U);
+    a.info = reinterpret_cast<int*>(d_info);
+    a.scratch = static_cast<double2*>(d->scratch);
+    a.batch = batch_size;
+    a.n = n;
+    a.ld = p.ld;
+    a.stage = 4;
+    const long long grid = batch_size < p.slots ? batch_size : p.slots;
+    geneig_plain_kernel<true, 0><<<(unsigned)grid, kNT, p.smem, reinterpret_cast<cudaStream_t>(stream)>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        api_set_error(std::string("sunny_geneig_launch_noalloc: kernel launch failed: ") + cudaGetErrorString(e));
+        return SUNNY_GENEIG_LAUNCH_ERROR;
+    }
+    return SUNNY_GENEIG_OK;
+}
+#pragma GCC visibility pop
