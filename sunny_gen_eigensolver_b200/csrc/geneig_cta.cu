@@ -44,9 +44,12 @@ struct CtaArgs {
 
 struct CtaVec {
     double2* tau;   // n   Householder scalars
-    double2* vb;    // n   current Householder vector
+    double2* vb;    // n   Householder vector of even steps
+    double2* vb2;   // n   Householder vector of odd steps (written one step ahead)
     double2* pb;    // n   tau * A22 * v
     double2* wred;  // 8   per-warp partial dots
+    double2* colv;  // 2n  column k of the Cholesky working matrix (double-buffered)
+    double2* rowv;  // 2n  row k of the inverse accumulator (double-buffered)
     double*  d;     // n
     double*  e;     // n
     double*  rdg;   // n   1 / L_kk
@@ -57,7 +60,7 @@ struct CtaVec {
 };
 
 __host__ __device__ inline size_t cta_vec_bytes(int n) {
-    return (size_t)n * 16 * 3 + 8 * 16 + (size_t)n * 8 * 3 + (size_t)dc_vec_doubles(n) * 8 +
+    return (size_t)n * 16 * 8 + 8 * 16 + (size_t)n * 8 * 3 + (size_t)dc_vec_doubles(n) * 8 +
            (size_t)dc_vec_ints(n) * 4 + (size_t)n * 4 + 8 * 4;
 }
 
@@ -65,9 +68,12 @@ __device__ inline CtaVec cta_carve(unsigned char* p, int n) {
     CtaVec v;
     v.tau  = reinterpret_cast<double2*>(p);
     v.vb   = v.tau + n;
-    v.pb   = v.vb + n;
+    v.vb2  = v.vb + n;
+    v.pb   = v.vb2 + n;
     v.wred = v.pb + n;
-    v.d    = reinterpret_cast<double*>(v.wred + 8);
+    v.colv = v.wred + 8;
+    v.rowv = v.colv + 2 * n;
+    v.d    = reinterpret_cast<double*>(v.rowv + 2 * n);
     v.e    = v.d + n;
     v.rdg  = v.e + n;
     v.dcd  = v.rdg + n;
@@ -117,50 +123,80 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             }
         if (tid < 8) v.ctl[tid] = 0;
 
-        // ---- a2: Cholesky, right-looking. Step k reads the unscaled column
-        // k (final after step k-1), updates the trailing lower triangle with
-        // a_ij -= a_ik conj(a_jk) / a_kk, and rescales column k-1 (no longer
-        // read by anyone) to L(:, k-1).
+        // ---- a2: Cholesky S = L L^H fused with X = L^-1, in registers.
+        // Group g owns row i = g; lane q holds slots j = q + 4t (t < R). Slot j
+        // holds the Cholesky working value a_ij while j > k and, from step j
+        // on, the inverse accumulator acc(i, j), so that at the end
+        // X(i, j) = acc(i, j) r_i with r_k = 1/sqrt(a_kk). Step k reads, from
+        // shared memory, column k (colv: a_jk, final after step k-1) and row k
+        // of acc (rowv: acc(k, j), j < k), and for i > k applies
+        //   a_ij -= a_ik conj(a_jk) r_k^2           k < j <= i
+        //   acc(i, j) -= a_ik r_k^2 acc(k, j)       j < k
+        //   acc(i, k) = -a_ik r_k^2
+        // then publishes column k+1 and row k+1 into the other buffers; one
+        // barrier per step. The step loop is unrolled so that slot k is a
+        // register known at compile time.
         int fail = 0;
-        double rprev = 0.0;
-        for (int k = 0; k < n; ++k) {
+        __syncthreads();   // the loads above are complete
+        {
+            const int i = g;
+            double2 x[R];
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int j = q + kG * t;
+                x[t] = (i < n && j <= i) ? A[i + (size_t)j * ld] : c2(0.0, 0.0);
+            }
+            if (i < n && q == 0) v.colv[i] = x[0];   // column 0, buffer 0
+            double ri = 0.0;
+#pragma unroll
+            for (int k = 0; k < NMAX; ++k) {
+                if (k >= n) break;
+                __syncthreads();
+                const double2* colk = v.colv + (k & 1) * n;
+                const double2* rowk = v.rowv + (k & 1) * n;
+                double2* coln = v.colv + ((k + 1) & 1) * n;
+                double2* rown = v.rowv + ((k + 1) & 1) * n;
+                const double akk = colk[k].x;
+                if (!(akk > 0.0)) { fail = k + 1; break; }   // uniform: every thread reads akk
+                const double r = rsqrt(akk);
+                const double r2 = r * r;
+                if (i == k) ri = r;
+                if (tid == 0) v.rdg[k] = r;
+                if (a.stage == 1) {   // stage-wise output: column k of L
+                    for (int jj = k + tid; jj < n; jj += kNT)
+                        A[jj + (size_t)k * ld] = (jj == k) ? c2(1.0 / r, 0.0) : cscale(colk[jj], r);
+                }
+                if (i > k && i < n) {
+                    const double2 aik = cscale(colk[i], r2);
+#pragma unroll
+                    for (int t = 0; t < R; ++t) {
+                        const int j = q + kG * t;
+                        if (j > k && j <= i) x[t] = cfms_bc(x[t], aik, colk[j]);
+                        else if (j < k) x[t] = cfms(x[t], aik, rowk[j]);
+                    }
+                    if (q == (k & 3)) x[k >> 2] = cscale(aik, -1.0);
+                }
+                // publish column k+1 (rows >= k+1) and row k+1 of acc (j <= k)
+                if (k + 1 < n) {
+                    if (i >= k + 1 && i < n && q == ((k + 1) & 3)) coln[i] = x[(k + 1) >> 2];
+                    if (i == k + 1) {
+#pragma unroll
+                        for (int t = 0; t < R; ++t) {
+                            const int j = q + kG * t;
+                            if (j <= k) rown[j] = x[t];
+                        }
+                    }
+                }
+            }
             __syncthreads();
-            const double akk = A[k + (size_t)k * ld].x;
-            if (!(akk > 0.0)) { fail = k + 1; break; }   // uniform: every thread reads akk
-            const double r = rsqrt(akk);
-            if (k > 0) {
-                const int c = k - 1;
-                for (int i = c + tid; i < n; i += kNT) {
-                    double2* p = A + i + (size_t)c * ld;
-                    *p = (i == c) ? c2(1.0 / rprev, 0.0) : cscale(*p, rprev);
+            if (!fail && a.stage >= 2 && i < n) {
+                // X(i, j) = acc(i, j) r_i, X(i, i) = r_i, into A's lower triangle
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    const int j = q + kG * t;
+                    if (j < i) A[i + (size_t)j * ld] = cscale(x[t], ri);
+                    else if (j == i) A[i + (size_t)i * ld] = c2(ri, 0.0);
                 }
-                if (tid == 0) v.rdg[c] = rprev;
-            }
-            // trailing update: group g takes row i = k+1+g (active rows map to the
-            // low groups, so finished rows leave whole warps idle); its four lanes
-            // take columns j = k+1+q, k+5+q, ... <= i
-            const double r2 = r * r;
-            const double2* ak = A + (size_t)k * ld;
-            const int i = k + 1 + g;
-            if (i < n) {
-                const double2 lik = cscale(ak[i], r2);
-                int j = k + 1 + q;
-                for (; j + 4 <= i; j += 8) {
-                    const double2 x0 = A[i + (size_t)j * ld], x1 = A[i + (size_t)(j + 4) * ld];
-                    const double2 l0 = ak[j], l1 = ak[j + 4];
-                    A[i + (size_t)j * ld] = cfms_bc(x0, lik, l0);
-                    A[i + (size_t)(j + 4) * ld] = cfms_bc(x1, lik, l1);
-                }
-                if (j <= i) A[i + (size_t)j * ld] = cfms_bc(A[i + (size_t)j * ld], lik, ak[j]);
-            }
-            rprev = r;
-        }
-        __syncthreads();
-        if (!fail) {
-            const int c = n - 1;
-            if (tid == 0) {
-                A[c + (size_t)c * ld] = c2(1.0 / rprev, 0.0);
-                v.rdg[c] = rprev;
             }
         }
         __syncthreads();
@@ -175,38 +211,6 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         }
 
         if (!code) {
-            // ---- X = L^-1 in place, right-looking over rows. At step k row k
-            // is finalised, X(k, j) = acc(k, j) / L_kk (group 0 did row k's last
-            // update at step k-1, with the same lane per column), then group g
-            // takes row i = k+1+g and subtracts L(i, k) X(k, :). acc(i, j) lives
-            // in the slot of L(i, j), whose last use is step j; at step k slot
-            // (i, k) receives -L(i, k) X(k, k) after all four lanes have read L(i, k).
-            for (int k = 0; k < n; ++k) {
-                if (g == 0) {
-                    const double rk = v.rdg[k];
-                    for (int j = q; j < k; j += kG) A[k + (size_t)j * ld] = cscale(A[k + (size_t)j * ld], rk);
-                    if (q == 0) A[k + (size_t)k * ld] = c2(rk, 0.0);
-                }
-                __syncthreads();
-                const int i = k + 1 + g;
-                if (i < n) {
-                    const double2 lik = A[i + (size_t)k * ld];
-                    __syncwarp(gmask);
-                    int j = q;
-                    for (; j + 4 < k; j += 8) {
-                        const double2 x0 = A[k + (size_t)j * ld], x1 = A[k + (size_t)(j + 4) * ld];
-                        const double2 a0 = A[i + (size_t)j * ld], a1 = A[i + (size_t)(j + 4) * ld];
-                        A[i + (size_t)j * ld] = cfms(a0, lik, x0);
-                        A[i + (size_t)(j + 4) * ld] = cfms(a1, lik, x1);
-                    }
-                    for (; j <= k; j += kG) {
-                        const double2 xkj = A[k + (size_t)j * ld];
-                        A[i + (size_t)j * ld] = (j == k) ? cscale(cmul(lik, xkj), -1.0)
-                                                         : cfms(A[i + (size_t)j * ld], lik, xkj);
-                    }
-                }
-            }
-            __syncthreads();
             // A now holds X = L^-1 in its lower triangle (diagonal real).
             // ---- a3: T = H X^H, T(i, j) = sum_{k <= j} H(i, k) conj(X(j, k))
             {
@@ -287,78 +291,101 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         if (!code) {
             // ---- a5a: Householder tridiagonalisation of C (lower). Reflector k:
             // I - tau_k v v^H on rows k+1.., v[k+1] = 1, v[k+2..] kept in A's
-            // strict upper triangle (row k), tau_k in v.tau.
-            for (int k = 0; k < n - 1; ++k) {
+            // strict upper triangle (row k), tau_k in v.tau. Look-ahead: during
+            // the rank-2 update of step k, warp 0 updates column k+1 first and
+            // computes reflector k+1 (into the other vector buffer) while warps
+            // 1-7 update the rest, so each step needs two barriers.
+            auto reflect = [&](int k, double2* vbuf) {   // warp 0
                 const double2* bk = B + (size_t)k * ld;
-                if (warp == 0) {
-                    double ss = 0.0;
-                    for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = bk[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
-                    ss = warp_sum(ss);
-                    const double2 alpha = bk[k + 1];
-                    double2 taui, scal = c2(0.0, 0.0);
-                    double beta;
-                    if (ss == 0.0 && alpha.y == 0.0) {
-                        taui = c2(0.0, 0.0);
-                        beta = alpha.x;
-                    } else {
-                        beta = -copysign(sqrt(fma(alpha.x, alpha.x, fma(alpha.y, alpha.y, ss))), alpha.x);
-                        const double rb = fast_rcp(beta);
-                        taui = c2((beta - alpha.x) * rb, -alpha.y * rb);
-                        const double2 z = c2(alpha.x - beta, alpha.y);
-                        const double inv = fast_rcp(fma(z.x, z.x, z.y * z.y));
-                        scal = c2(z.x * inv, -z.y * inv);
-                    }
-                    for (int i = k + 2 + lane; i < n; i += 32) {
-                        const double2 vi = cmul(bk[i], scal);
-                        v.vb[i] = vi;
-                        A[k + (size_t)i * ld] = vi;
-                    }
-                    if (lane == 0) {
-                        v.vb[k + 1] = c2(1.0, 0.0);
-                        v.tau[k] = taui;
-                        v.d[k] = bk[k].x;
-                        v.e[k] = beta;
-                    }
+                double ss = 0.0;
+                for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = bk[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                ss = warp_sum(ss);
+                const double2 alpha = bk[k + 1];
+                double2 taui, scal = c2(0.0, 0.0);
+                double beta;
+                if (ss == 0.0 && alpha.y == 0.0) {
+                    taui = c2(0.0, 0.0);
+                    beta = alpha.x;
+                } else {
+                    beta = -copysign(sqrt(fma(alpha.x, alpha.x, fma(alpha.y, alpha.y, ss))), alpha.x);
+                    const double rb = fast_rcp(beta);
+                    taui = c2((beta - alpha.x) * rb, -alpha.y * rb);
+                    const double2 z = c2(alpha.x - beta, alpha.y);
+                    const double inv = fast_rcp(fma(z.x, z.x, z.y * z.y));
+                    scal = c2(z.x * inv, -z.y * inv);
                 }
-                __syncthreads();
+                for (int i = k + 2 + lane; i < n; i += 32) {
+                    const double2 vi = cmul(bk[i], scal);
+                    vbuf[i] = vi;
+                    A[k + (size_t)i * ld] = vi;
+                }
+                if (lane == 0) {
+                    vbuf[k + 1] = c2(1.0, 0.0);
+                    v.tau[k] = taui;
+                    v.d[k] = bk[k].x;
+                    v.e[k] = beta;
+                }
+            };
+            if (n >= 2 && warp == 0) reflect(0, v.vb);
+            __syncthreads();
+            for (int k = 0; k < n - 1; ++k) {
+                double2* vk = (k & 1) ? v.vb2 : v.vb;
+                double2* vn = (k & 1) ? v.vb : v.vb2;
                 const double2 taui = v.tau[k];
-                if (taui.x == 0.0 && taui.y == 0.0) continue;
-                // p = tau A22 v: four lanes per row; per-warp partial of p^H v
-                {
+                const bool has = !(taui.x == 0.0 && taui.y == 0.0);
+                if (has) {
+                    // p = tau A22 v: four lanes per row; per-warp partial of p^H v
                     double2 dotp = c2(0.0, 0.0);
                     for (int i = k + 1 + g; i < n; i += kNG) {
                         double2 acc = c2(0.0, 0.0);
-                        for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], v.vb[j]);
+                        for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], vk[j]);
                         acc = group_sum2<kG>(gmask, acc);
                         const double2 pi = cmul(taui, acc);
-                        if (q == 0) { v.pb[i] = pi; dotp = cfmac(dotp, pi, v.vb[i]); }
+                        if (q == 0) { v.pb[i] = pi; dotp = cfmac(dotp, pi, vk[i]); }
                     }
                     dotp = warp_sum2(dotp);
                     if (lane == 0) v.wred[warp] = dotp;
+                    __syncthreads();
                 }
-                __syncthreads();
-                // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v);
-                // group g takes row i = k+1+g, its lanes columns j = k+1+q step 4
-                {
+                // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v)
+                double2 alpha2 = c2(0.0, 0.0);
+                if (has) {
                     double2 dot = c2(0.0, 0.0);
 #pragma unroll
                     for (int w = 0; w < kNT / 32; ++w) dot = cadd(dot, v.wred[w]);
-                    const double2 alpha2 = cscale(cmul(taui, dot), -0.5);
-                    const int i = k + 1 + g;
-                    if (i < n) {
-                        const double2 vi = v.vb[i];
+                    alpha2 = cscale(cmul(taui, dot), -0.5);
+                }
+                if (warp == 0) {
+                    if (has) {
+                        const int j = k + 1;
+                        const double2 vj = vk[j];
+                        const double2 wj = cfma(v.pb[j], alpha2, vj);
+                        for (int i = j + lane; i < n; i += 32) {
+                            const double2 vi = vk[i];
+                            const double2 wi = cfma(v.pb[i], alpha2, vi);
+                            double2* p = B + i + (size_t)j * ld;
+                            *p = cfms_bc(cfms_bc(*p, vi, wj), wi, vj);
+                        }
+                        __syncwarp();
+                    }
+                    if (k + 1 < n - 1) reflect(k + 1, vn);
+                } else if (has) {
+                    // group g - 8 of warps 1-7 takes rows k+1+(g-8), +56, ...;
+                    // its lanes take columns j = k+2+q step 4 (column k+1 is warp 0's)
+                    for (int i = k + 1 + (g - 8); i < n; i += kNG - 8) {
+                        const double2 vi = vk[i];
                         const double2 wi = cfma(v.pb[i], alpha2, vi);
                         double2* bi = B + i;
-                        int j = k + 1 + q;
+                        int j = k + 2 + q;
                         for (; j + 4 < n; j += 8) {
                             const double2 x0 = bi[(size_t)j * ld], x1 = bi[(size_t)(j + 4) * ld];
-                            const double2 v0 = v.vb[j], v1 = v.vb[j + 4];
+                            const double2 v0 = vk[j], v1 = vk[j + 4];
                             const double2 w0 = cfma(v.pb[j], alpha2, v0), w1 = cfma(v.pb[j + 4], alpha2, v1);
                             bi[(size_t)j * ld] = cfms_bc(cfms_bc(x0, vi, w0), wi, v0);
                             bi[(size_t)(j + 4) * ld] = cfms_bc(cfms_bc(x1, vi, w1), wi, v1);
                         }
                         if (j < n) {
-                            const double2 v0 = v.vb[j];
+                            const double2 v0 = vk[j];
                             const double2 w0 = cfma(v.pb[j], alpha2, v0);
                             bi[(size_t)j * ld] = cfms_bc(cfms_bc(bi[(size_t)j * ld], vi, w0), wi, v0);
                         }

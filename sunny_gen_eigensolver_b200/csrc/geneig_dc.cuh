@@ -150,19 +150,19 @@ __host__ __device__ inline int secular_root_p(int i, int K, const double* dl, co
             const double C = bpsi * q + bphi * p;
             tn = lo - 1.0;
             if (c == 0.0) {
-                tn = -C / B;
+                tn = -C * fast_rcp(B);
             } else {
                 double disc = B * B - 4.0 * c * C;
                 if (disc < 0.0) disc = 0.0;
                 const double qq2 = -0.5 * (B + copysign(sqrt(disc), B));
-                const double x1 = qq2 / c, x2 = (qq2 != 0.0) ? C / qq2 : x1;
+                const double x1 = qq2 * fast_rcp(c), x2 = (qq2 != 0.0) ? C * fast_rcp(qq2) : x1;
                 tn = (x1 > lo && x1 < hi) ? x1 : x2;
             }
         } else {
             const double bpsi = dpsi * (p - tau) * (p - tau);
             const double apsi = psi - dpsi * (p - tau);
             const double den = 1.0 + apsi;
-            tn = (den > 0.0) ? p + bpsi / den : lo - 1.0;
+            tn = (den > 0.0) ? p + bpsi * fast_rcp(den) : lo - 1.0;
         }
         // converged when the model step is within a few ulps of the iterate
         // (it may then round just outside the bracket)
