@@ -91,6 +91,68 @@ __device__ __forceinline__ void tile_zero(double2 (&acc)[TM][TM]) {
         for (int b = 0; b < TM; ++b) acc[a][b] = c2(0.0, 0.0);
 }
 
+// One FP64 tensor-core step D += A B on an 8x8x4 tile (mma.m8n8k4.f64).
+// Fragments: lane l holds A(l/4, l%4), B(l%4, l/4) and D(l/4, 2(l%4)+{0,1}).
+__device__ __forceinline__ void mma884(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+// Complex product on 8x8 output tiles, one warp per tile (round robin over
+// the CTA's warps), four real MMAs per 8x8x4 step:
+//   Dr += Ar Br - Ai Bi,  Di += Ar Bi + Ai Br.
+// fa(i, k) / fb(k, j) return the operands (zero outside their nonzero
+// pattern and outside the matrix); kr(ti, tj, k0, k1) bounds the k loop of
+// tile (ti, tj); keep(ti, tj) selects the tiles to compute. The results stay
+// in registers (acc) so that the caller can barrier before overwriting an
+// operand, then call `put` for every computed element.
+template <int MAXT>
+struct ZTiles {
+    double re[MAXT][2], im[MAXT][2];
+};
+
+template <int MAXT, class FA, class FB, class FK, class FKeep>
+__device__ __forceinline__ void ztiles_compute(ZTiles<MAXT>& acc, int tm, int tn, FA fa, FB fb, FK kr, FKeep keep) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = kNT / 32;
+#pragma unroll
+    for (int u = 0; u < MAXT; ++u) {
+        acc.re[u][0] = acc.re[u][1] = acc.im[u][0] = acc.im[u][1] = 0.0;
+        const int t = warp + NW * u;
+        if (t >= tm * tn) continue;
+        const int ti = t / tn, tj = t - ti * tn;
+        if (!keep(ti, tj)) continue;
+        int k0, k1;
+        kr(ti, tj, k0, k1);
+        const int ia = 8 * ti + (lane >> 2), ka = lane & 3;   // A fragment element
+        const int kb = lane & 3, jb = 8 * tj + (lane >> 2);   // B fragment element
+        for (int k = k0; k < k1; k += 4) {
+            const double2 av = fa(ia, k + ka);
+            const double2 bv = fb(k + kb, jb);
+            mma884(acc.re[u][0], acc.re[u][1], av.x, bv.x);
+            mma884(acc.re[u][0], acc.re[u][1], -av.y, bv.y);
+            mma884(acc.im[u][0], acc.im[u][1], av.x, bv.y);
+            mma884(acc.im[u][0], acc.im[u][1], av.y, bv.x);
+        }
+    }
+}
+
+template <int MAXT, class FKeep, class FPut>
+__device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, int tn, FKeep keep, FPut put) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = kNT / 32;
+#pragma unroll
+    for (int u = 0; u < MAXT; ++u) {
+        const int t = warp + NW * u;
+        if (t >= tm * tn) continue;
+        const int ti = t / tn, tj = t - ti * tn;
+        if (!keep(ti, tj)) continue;
+        const int i = 8 * ti + (lane >> 2), j = 8 * tj + 2 * (lane & 3);
+        put(i, j, c2(acc.re[u][0], acc.im[u][0]));
+        put(i, j + 1, c2(acc.re[u][1], acc.im[u][1]));
+    }
+}
+
 template <int NMAX>
 __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(CtaArgs a) {
     constexpr int TM = NMAX / 16;   // register tile edge
@@ -212,71 +274,41 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
 
         if (!code) {
             // A now holds X = L^-1 in its lower triangle (diagonal real).
-            // ---- a3: T = H X^H, T(i, j) = sum_{k <= j} H(i, k) conj(X(j, k))
+            // ---- a3: T = H X^H, T(i, j) = sum_{k <= j} H(i, k) conj(X(j, k)),
+            // FP64 tensor-core tiles; T overwrites H after the barrier.
+            constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + kNT / 32 - 1) / (kNT / 32);
+            const int tn8 = (n + 7) >> 3;
             {
-                double2 acc[TM][TM];
-                tile_zero<TM>(acc);
-                int kmax = tc + 16 * (TM - 1);
-                if (kmax > n - 1) kmax = n - 1;
-                for (int k = 0; k <= kmax; ++k) {
-                    double2 hv[TM], xv[TM];
-                    const double2* bk = B + (size_t)k * ld;
-#pragma unroll
-                    for (int t = 0; t < TM; ++t) {
-                        const int i = tr + 16 * t, j = tc + 16 * t;
-                        hv[t] = (i < n) ? bk[i] : c2(0.0, 0.0);
-                        xv[t] = (j < n && k <= j) ? cconj(A[j + (size_t)k * ld]) : c2(0.0, 0.0);
-                    }
-#pragma unroll
-                    for (int aa = 0; aa < TM; ++aa)
-#pragma unroll
-                        for (int bb = 0; bb < TM; ++bb) acc[aa][bb] = cfma(acc[aa][bb], hv[aa], xv[bb]);
-                }
+                ZTiles<MAXT> acc;
+                ztiles_compute<MAXT>(acc, tn8, tn8,
+                    [&](int i, int k) { return (i < n && k < n) ? B[i + (size_t)k * ld] : c2(0.0, 0.0); },
+                    [&](int k, int j) { return (j < n && k <= j) ? cconj(A[j + (size_t)k * ld]) : c2(0.0, 0.0); },
+                    [&](int, int tj, int& k0, int& k1) { k0 = 0; k1 = min(n, 8 * tj + 8); },
+                    [](int, int) { return true; });
                 __syncthreads();
-#pragma unroll
-                for (int aa = 0; aa < TM; ++aa)
-#pragma unroll
-                    for (int bb = 0; bb < TM; ++bb) {
-                        const int i = tr + 16 * aa, j = tc + 16 * bb;
-                        if (i < n && j < n) B[i + (size_t)j * ld] = acc[aa][bb];
-                    }
+                ztiles_store<MAXT>(acc, tn8, tn8, [](int, int) { return true; },
+                    [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
                 __syncthreads();
             }
-            // ---- a4: C = X T, C(i, j) = sum_{k <= i} X(i, k) T(k, j); keep the
-            // lower triangle and mirror it, so that C is exactly Hermitian.
+            // ---- a4: C = X T, C(i, j) = sum_{k <= i} X(i, k) T(k, j); lower
+            // tiles only, each lower element written with its mirror, so that
+            // C is exactly Hermitian.
             {
-                double2 acc[TM][TM];
-                tile_zero<TM>(acc);
-                int kmax = tr + 16 * (TM - 1);
-                if (kmax > n - 1) kmax = n - 1;
-                for (int k = 0; k <= kmax; ++k) {
-                    double2 xv[TM], tv[TM];
-                    const double2* xk = A + (size_t)k * ld;
-                    const double2* tk = B + k;
-#pragma unroll
-                    for (int t = 0; t < TM; ++t) {
-                        const int i = tr + 16 * t, j = tc + 16 * t;
-                        xv[t] = (i < n && k <= i) ? xk[i] : c2(0.0, 0.0);
-                        tv[t] = (j < n) ? tk[(size_t)j * ld] : c2(0.0, 0.0);
-                    }
-#pragma unroll
-                    for (int aa = 0; aa < TM; ++aa)
-#pragma unroll
-                        for (int bb = 0; bb < TM; ++bb) acc[aa][bb] = cfma(acc[aa][bb], xv[aa], tv[bb]);
-                }
+                ZTiles<MAXT> acc;
+                ztiles_compute<MAXT>(acc, tn8, tn8,
+                    [&](int i, int k) { return (i < n && k <= i) ? A[i + (size_t)k * ld] : c2(0.0, 0.0); },
+                    [&](int k, int j) { return (k < n && j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0); },
+                    [&](int ti, int, int& k0, int& k1) { k0 = 0; k1 = min(n, 8 * ti + 8); },
+                    [](int ti, int tj) { return ti >= tj; });
                 __syncthreads();
-#pragma unroll
-                for (int aa = 0; aa < TM; ++aa)
-#pragma unroll
-                    for (int bb = 0; bb < TM; ++bb) {
-                        const int i = tr + 16 * aa, j = tc + 16 * bb;
+                ztiles_store<MAXT>(acc, tn8, tn8, [](int ti, int tj) { return ti >= tj; },
+                    [&](int i, int j, double2 c) {
                         if (i < n && j < n && i >= j) {
-                            double2 c = acc[aa][bb];
                             if (i == j) c.y = 0.0;
                             B[i + (size_t)j * ld] = c;
                             B[j + (size_t)i * ld] = cconj(c);
                         }
-                    }
+                    });
                 __syncthreads();
             }
         }
@@ -492,31 +524,20 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             if (tid == 0) a.info[b] = 0;
             continue;
         }
-        // ---- a6: U = X^H V, U(i, j) = sum_{k >= i} conj(X(k, i)) V(k, j)
+        // ---- a6: U = X^H V, U(i, j) = sum_{k >= i} conj(X(k, i)) V(k, j), FP64
+        // tensor-core tiles; U overwrites V after the barrier.
         {
-            double2 acc[TM][TM];
-            tile_zero<TM>(acc);
-            for (int k = tr; k < n; ++k) {
-                double2 xv[TM], vv[TM];
-#pragma unroll
-                for (int t = 0; t < TM; ++t) {
-                    const int i = tr + 16 * t, j = tc + 16 * t;
-                    xv[t] = (i < n && k >= i) ? cconj(A[k + (size_t)i * ld]) : c2(0.0, 0.0);
-                    vv[t] = (j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0);
-                }
-#pragma unroll
-                for (int aa = 0; aa < TM; ++aa)
-#pragma unroll
-                    for (int bb = 0; bb < TM; ++bb) acc[aa][bb] = cfma(acc[aa][bb], xv[aa], vv[bb]);
-            }
+            constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + kNT / 32 - 1) / (kNT / 32);
+            const int tn8 = (n + 7) >> 3;
+            ZTiles<MAXT> acc;
+            ztiles_compute<MAXT>(acc, tn8, tn8,
+                [&](int i, int k) { return (i < n && k >= i && k < n) ? cconj(A[k + (size_t)i * ld]) : c2(0.0, 0.0); },
+                [&](int k, int j) { return (k < n && j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0); },
+                [&](int ti, int, int& k0, int& k1) { k0 = 8 * ti; k1 = n; },
+                [](int, int) { return true; });
             __syncthreads();
-#pragma unroll
-            for (int aa = 0; aa < TM; ++aa)
-#pragma unroll
-                for (int bb = 0; bb < TM; ++bb) {
-                    const int i = tr + 16 * aa, j = tc + 16 * bb;
-                    if (i < n && j < n) B[i + (size_t)j * ld] = acc[aa][bb];
-                }
+            ztiles_store<MAXT>(acc, tn8, tn8, [](int, int) { return true; },
+                [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
             __syncthreads();
         }
         // ---- a7: store U, column j to position rank[j]
