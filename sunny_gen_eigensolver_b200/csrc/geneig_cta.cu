@@ -4,22 +4,21 @@
 //
 // Stage chain (reference: src/unified/kernel_source.hpp:233-276):
 //   a1  load S -> A, H -> B                                   (:233-242)
-//   a2  Cholesky S = L L^H, right-looking, one barrier per column  (:244)
-//       then L^-1 in place (forward substitution on I, rows owned by
-//       groups of four lanes)
-//   a3+a4  C = L^-1 H L^-H as two register-tiled GEMMs with X = L^-1:
-//       T = H X^H, then C = X T (lower triangle kept and mirrored); H is
-//       read in full, as the reference's two triangular solves do (:246-248)
-//   a5  Householder tridiagonalisation (lower), divide and conquer on the
-//       tridiagonal, back-transform V = Q Z in registers per column (:250)
-//   a6  U = L^-H V as a register-tiled GEMM                    (:252)
+//   a2  Cholesky S = L L^H fused with X = L^-1: each row lives in the
+//       registers of a four-lane group, one barrier per column   (:244)
+//   a3+a4  C = L^-1 H L^-H as two complex GEMMs on the FP64 tensor cores
+//       (mma.m8n8k4.f64): T = H X^H, then C = X T (lower tiles, mirrored);
+//       H is read in full, as the reference's two triangular solves do (:246-248)
+//   a5  Householder tridiagonalisation (lower, look-ahead reflector, two
+//       barriers per step), divide and conquer on the tridiagonal,
+//       back-transform V = Q Z in registers per column        (:250)
+//   a6  U = L^-H V = X^H V on the FP64 tensor cores            (:252)
 //   a7  W (ascending) and U, columns permuted by eigenvalue rank (:268-276)
 //
-// Thread layouts (NT = 256): a 16 x 16 grid (tr = tid / 16, tc = tid % 16)
-// owning TM x TM register tiles (rows tr + 16 a, columns tc + 16 b) for the
-// GEMMs and the Householder rank-2 updates; groups of four lanes
-// (g = tid / 4, q = tid % 4) owning one row or one column for the
-// substitutions and the back-transform.
+// Thread layouts (NT = 256): groups of four lanes (g = tid / 4, q = tid % 4)
+// owning one row or one column for the Cholesky/inverse, the Householder
+// updates and the back-transform; warps owning 8x8 output tiles for the
+// tensor-core GEMMs; a 16 x 16 grid (tr, tc) for the copies.
 
 #include "geneig_common.cuh"
 #include "geneig_dc.cuh"
@@ -81,14 +80,6 @@ __device__ inline CtaVec cta_carve(unsigned char* p, int n) {
     v.rank = v.dci + dc_vec_ints(n);
     v.ctl  = v.rank + n;
     return v;
-}
-
-template <int TM>
-__device__ __forceinline__ void tile_zero(double2 (&acc)[TM][TM]) {
-#pragma unroll
-    for (int a = 0; a < TM; ++a)
-#pragma unroll
-        for (int b = 0; b < TM; ++b) acc[a][b] = c2(0.0, 0.0);
 }
 
 // One FP64 tensor-core step D += A B on an 8x8x4 tile (mma.m8n8k4.f64).
@@ -155,7 +146,6 @@ __device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, in
 
 template <int NMAX>
 __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(CtaArgs a) {
-    constexpr int TM = NMAX / 16;   // register tile edge
     constexpr int R = NMAX / kG;    // rows per lane in a column group
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = a.n, ld = a.ld;

@@ -376,43 +376,37 @@ __device__ void tridiag_dc(int n, DCShared s) {
         __syncthreads();
         // ---- phase E: Z(:, nd) <- Z(:, nd) * U.
         if (span >= n) {
-            // one merge over [0, n): 16 x 16 threads with register tiles
-            // (rows tr + 16 x, output columns tc + 16 y); all reads finish
-            // before the barrier, then the tiles are written back.
-            constexpr int TM = NMAX / 16;
-            const int tr = tid >> 4, tc = tid & 15;
+            // one merge over [0, n): 8x8 output tiles on the FP64 tensor cores
+            // (mma.m8n8k4.f64), one warp per tile; all reads finish before the
+            // barrier, then the tiles are written back to the gathered columns.
             const int K = s.kcnt[0];
-            double acc[TM][TM];
+            const int tm = (n + 7) >> 3, tn = (K + 7) >> 3;
+            constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + NW - 1) / NW;
+            double acc[MAXT][2];
 #pragma unroll
-            for (int x = 0; x < TM; ++x)
-#pragma unroll
-                for (int y = 0; y < TM; ++y) acc[x][y] = 0.0;
-            if (K > 0) {
-                for (int l = 0; l < K; ++l) {
-                    const double* zc = s.Z + (size_t)s.nd[l] * s.ldz;
-                    const double* ur = s.U + l;
-                    double zr[TM], uc[TM];
-#pragma unroll
-                    for (int t = 0; t < TM; ++t) {
-                        const int r = tr + 16 * t, j = tc + 16 * t;
-                        zr[t] = (r < n) ? zc[r] : 0.0;
-                        uc[t] = (j < K) ? ur[(size_t)j * s.ldu] : 0.0;
-                    }
-#pragma unroll
-                    for (int x = 0; x < TM; ++x)
-#pragma unroll
-                        for (int y = 0; y < TM; ++y) acc[x][y] = fma(zr[x], uc[y], acc[x][y]);
+            for (int u = 0; u < MAXT; ++u) {
+                acc[u][0] = acc[u][1] = 0.0;
+                const int t = warp + NW * u;
+                if (K == 0 || t >= tm * tn) continue;
+                const int ti = t / tn, tj = t - ti * tn;
+                const int ia = 8 * ti + (lane >> 2), jb = 8 * tj + (lane >> 2);
+                for (int k = 0; k < K; k += 4) {
+                    const int ka = k + (lane & 3);
+                    const double av = (ia < n && ka < K) ? s.Z[ia + (size_t)s.nd[ka] * s.ldz] : 0.0;
+                    const double bv = (ka < K && jb < K) ? s.U[ka + (size_t)jb * s.ldu] : 0.0;
+                    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                        : "+d"(acc[u][0]), "+d"(acc[u][1]) : "d"(av), "d"(bv));
                 }
             }
             __syncthreads();
-            if (K > 0) {
 #pragma unroll
-                for (int x = 0; x < TM; ++x)
-#pragma unroll
-                    for (int y = 0; y < TM; ++y) {
-                        const int r = tr + 16 * x, j = tc + 16 * y;
-                        if (r < n && j < K) s.Z[r + (size_t)s.nd[j] * s.ldz] = acc[x][y];
-                    }
+            for (int u = 0; u < MAXT; ++u) {
+                const int t = warp + NW * u;
+                if (K == 0 || t >= tm * tn) continue;
+                const int ti = t / tn, tj = t - ti * tn;
+                const int r = 8 * ti + (lane >> 2), j = 8 * tj + 2 * (lane & 3);
+                if (r < n && j < K) s.Z[r + (size_t)s.nd[j] * s.ldz] = acc[u][0];
+                if (r < n && j + 1 < K) s.Z[r + (size_t)s.nd[j + 1] * s.ldz] = acc[u][1];
             }
         } else {
             // several merges, each of at most `span` columns, span being at most
