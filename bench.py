@@ -191,11 +191,12 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    from sunny_gen_eigensolver_b200 import Solver
+    from sunny_gen_eigensolver_b200 import Solver, replicas
     from sunny_gen_eigensolver_b200.generators import baseline_problems_torch
 
     n, batch = args.n, args.batch
-    H, S = baseline_problems_torch(n, batch, seed=20261203 + 1 + rank, kappa=args.kappa, device=dev)
+    H, S = baseline_problems_torch(n, batch, seed=replicas.rank_seed(20261203 + 1, rank), kappa=args.kappa,
+                                   device=dev)
     H = H.transpose(-1, -2).contiguous()   # column-major buffers (Julia layout)
     S = S.transpose(-1, -2).contiguous()
     W = torch.empty((batch, n), dtype=torch.float64, device=dev)
@@ -207,10 +208,7 @@ def run_ours(args):
     peak = measure_fp64_peak(torch, dev)
 
     def barrier():
-        if world > 1:
-            t = torch.zeros(1, device=dev)
-            dist.all_reduce(t)
-        torch.cuda.synchronize(dev)
+        replicas.barrier(dev)
 
     for _ in range(args.warmup):
         solver.launch(H, S, W, U, info, stream)
@@ -227,10 +225,7 @@ def run_ours(args):
         t1.record(stream)
         barrier()
     elapsed = t0.elapsed_time(t1) * 1e-3
-    el_t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
-    elapsed_max = float(el_t.item())
+    elapsed_max = replicas.max_over_ranks(elapsed, dev)
     clocks = clk.summary()
 
     # accuracy of the last step's results (all matrices, on the device)
