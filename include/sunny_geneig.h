@@ -91,7 +91,10 @@ void sunny_geneig_destroy(sunny_geneig_solver_t solver);
 /* replaces src/common/c_api.h:77-85 (impl c_api.cpp:147-186).
  * INVALID_ARG for a NULL solver, batch_size < 0, a NULL or misaligned
  * buffer with batch_size > 0; batch_size == 0 is a no-op returning OK;
- * LAUNCH_ERROR when the CUDA launch itself fails. */
+ * LAUNCH_ERROR when the CUDA launch itself fails. One handle may be used
+ * from several streams: for sizes whose solver keeps scratch slots (the
+ * "l2-slot" regime) a launch on a different stream than the previous one
+ * waits for it on the device, so launches of one such handle never overlap. */
 sunny_geneig_status_t sunny_geneig_launch(
     sunny_geneig_solver_t solver,
     uintptr_t             d_H,

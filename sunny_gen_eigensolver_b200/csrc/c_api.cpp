@@ -13,6 +13,7 @@
 
 #include <cstdint>
 #include <exception>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -25,6 +26,13 @@ struct sunny_geneig_solver {
     int bpb = 1;
     sgeig::PlainPlan plan;
     void* scratch = nullptr;
+    // Scratch ordering across streams: a launch that uses the handle's
+    // scratch slots waits for the previous such launch when that one went to
+    // another stream (launches on one stream are ordered by the stream).
+    cudaEvent_t scratch_done = nullptr;
+    uintptr_t last_stream = 0;
+    bool scratch_used = false;
+    std::mutex scratch_mu;
 };
 
 namespace {
@@ -97,12 +105,15 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
         if (s->plan.scratch_bytes) {
             cudaError_t ea = cudaMalloc(&s->scratch, s->plan.scratch_bytes);
             if (ea != cudaSuccess) { err = std::string("cudaMalloc scratch: ") + cudaGetErrorString(ea); return ea; }
+            ea = cudaEventCreateWithFlags(&s->scratch_done, cudaEventDisableTiming);
+            if (ea != cudaSuccess) { err = std::string("cudaEventCreate: ") + cudaGetErrorString(ea); return ea; }
         }
         return cudaSuccess;
     });
     if (e != cudaSuccess) {
         set_error(std::string(fn) + ": " + (err.empty() ? cudaGetErrorString(e) : err));
         if (s->scratch) with_device(device_id, [&]() { return cudaFree(s->scratch); });
+        if (s->scratch_done) with_device(device_id, [&]() { return cudaEventDestroy(s->scratch_done); });
         delete s;
         return nullptr;
     }
@@ -126,12 +137,30 @@ sunny_geneig_status_t launch_impl(sunny_geneig_solver_t s, int stage, uintptr_t 
         return SUNNY_GENEIG_INVALID_ARG;
     }
     try {
-        cudaError_t e = with_device(s->device, [&]() {
+        auto run = [&]() {
             return sgeig::plain_launch(s->plan, stage, reinterpret_cast<const void*>(d_H),
                                        reinterpret_cast<const void*>(d_S), reinterpret_cast<double*>(d_W),
                                        reinterpret_cast<void*>(d_U), reinterpret_cast<int*>(d_info), batch,
                                        s->scratch, reinterpret_cast<cudaStream_t>(stream));
-        });
+        };
+        cudaError_t e;
+        if (s->scratch) {
+            std::lock_guard<std::mutex> lock(s->scratch_mu);
+            e = with_device(s->device, [&]() {
+                const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+                if (s->scratch_used && s->last_stream != stream) {
+                    cudaError_t w = cudaStreamWaitEvent(st, s->scratch_done, 0);
+                    if (w != cudaSuccess) return w;
+                }
+                cudaError_t l = run();
+                if (l != cudaSuccess) return l;
+                l = cudaEventRecord(s->scratch_done, st);
+                if (l == cudaSuccess) { s->scratch_used = true; s->last_stream = stream; }
+                return l;
+            });
+        } else {
+            e = with_device(s->device, run);
+        }
         if (e != cudaSuccess) {
             set_error(std::string(fn) + ": kernel launch failed: " + cudaGetErrorString(e));
             return SUNNY_GENEIG_LAUNCH_ERROR;
@@ -187,7 +216,12 @@ void sunny_geneig_destroy(sunny_geneig_solver_t solver) {
         if (solver->scratch) {
             const int dev = solver->device;
             void* p = solver->scratch;
-            with_device(dev, [&]() { return cudaFree(p); });
+            cudaEvent_t ev = solver->scratch_done;
+            with_device(dev, [&]() {
+                if (ev) cudaEventSynchronize(ev);   // no launch may still use the slots
+                if (ev) cudaEventDestroy(ev);
+                return cudaFree(p);
+            });
         }
         delete solver;
     } catch (...) {

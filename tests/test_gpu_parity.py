@@ -71,6 +71,13 @@ def test_baseline_generator_sizes(cuda, n):
     check_against_zhegv(H, S, W, U, info)
 
 
+@pytest.mark.parametrize("n", [162, 216, 384])
+def test_large_sizes_l2_slot(cuda, n):
+    H, S = generators.baseline_problems(n, 2, seed=97 + n)
+    W, U, info = gpu_solve(H, S)
+    check_against_zhegv(H, S, W, U, info)
+
+
 @pytest.mark.parametrize("n", [1, 3, 5, 7, 33, 55])
 def test_odd_sizes(cuda, n):
     rng = np.random.default_rng(n)
@@ -210,3 +217,30 @@ def test_abi_errors_on_gpu(cuda):
         assert s.path_name == "unified" and s.kernel_mode == "unified"
     with Solver(16, kernel="hybrid") as s:
         assert s.path_name == "hybrid"
+
+
+def test_one_l2_slot_handle_on_two_streams(cuda):
+    """A handle whose solver keeps scratch slots, launched from two streams
+    back to back: the second launch must not overlap the first on the slots."""
+    import torch
+    from sunny_gen_eigensolver_b200 import Solver, to_colmajor
+    n = 108
+    H, S = generators.baseline_problems(n, 24, seed=5150)
+    Ht, St = to_colmajor(torch.from_numpy(H).cuda()), to_colmajor(torch.from_numpy(S).cuda())
+    with Solver(n) as s:
+        assert s.regime == "l2-slot"
+        Wr, Ur, ir = s.run_kernel(Ht, St)
+        torch.cuda.synchronize()
+        s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+        outs = []
+        for rep in range(3):
+            for st, sl in ((s1, slice(0, 12)), (s2, slice(12, 24))):
+                W = torch.empty((12, n), dtype=torch.float64, device="cuda")
+                U = torch.empty((12, n, n), dtype=torch.complex128, device="cuda")
+                info = torch.empty((12,), dtype=torch.int32, device="cuda")
+                with torch.cuda.stream(st):
+                    s.launch(Ht[sl], St[sl], W, U, info, st)
+                outs.append((sl, W, U, info))
+        torch.cuda.synchronize()
+        for sl, W, U, info in outs:
+            assert torch.equal(W, Wr[sl]) and torch.equal(U, Ur[sl]) and torch.equal(info, ir[sl])
