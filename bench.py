@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--e2e-chunk", type=int, default=8192)
     p.add_argument("--serving", action="store_true", help="run the serving-loop workload instead")
+    p.add_argument("--uneven", action="store_true", help="run the uneven-size batch workload instead")
+    p.add_argument("--uneven-total", type=int, default=200000, help="uneven: number of problems")
     p.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate (req/s)")
     p.add_argument("--duration", type=float, default=10.0, help="serving: arrival window (s)")
     p.add_argument("--sizes", type=str, default="18,54,108,216,384", help="serving: matrix sizes")
@@ -371,12 +373,63 @@ def run_serving(args):
     print(json.dumps(out), flush=True)
 
 
+def run_uneven(args):
+    """Uneven-size batch: problems with N drawn from {12,24,54,72,108,162,216}
+    (30/20/25/10/8/5/2 %), packed per size, all sizes in one CUDA graph launch
+    (autotuned stream plan) vs one plain launch per size on one stream."""
+    import numpy as np
+    import torch
+    from sunny_gen_eigensolver_b200.batching import TuneTable, UnevenBatch
+    from sunny_gen_eigensolver_b200.generators import baseline_problems_torch
+    sizes_set = [12, 24, 54, 72, 108, 162, 216]
+    weights = [0.30, 0.20, 0.25, 0.10, 0.08, 0.05, 0.02]
+    rng = np.random.default_rng(20261205)
+    sizes = rng.choice(sizes_set, size=args.uneven_total, p=weights)
+    ub = UnevenBatch(sizes)
+    for n, c in ub.counts.items():
+        H, S = baseline_problems_torch(n, c, seed=3000 + n, kappa=args.kappa)
+        ub.set_inputs(n, H.transpose(-1, -2), S.transpose(-1, -2))
+        del H, S
+    torch.cuda.synchronize()
+    table = TuneTable(Path(tempfile.gettempdir()) / "sunny_geneig_bench_plans.json")
+    plan = ub.autotune(table)
+
+    def timed(fn, k):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3 / k
+
+    steps = max(1, args.steps // 4)
+    t_graph = timed(ub.replay, steps)
+    t_seq = timed(ub.run_sequential, steps)
+    bad = sum(int((ub.info[n] != 0).sum().item()) for n in ub.counts)
+    flops = sum(flops_per_solve(n) * c for n, c in ub.counts.items())
+    out = {"metric": METRIC, "mode": "uneven", "value": ub.total / t_graph, "unit": "solves/s",
+           "ms_per_step": 1e3 * t_graph, "steps": steps, "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+           "data": "synthetic (seeded BdG H / Haar-unitary S per size)",
+           "config": {"workload": "uneven-size persistent batch", "total": ub.total,
+                      "counts": {str(n): c for n, c in ub.counts.items()}},
+           "graph_solves_per_s": ub.total / t_graph, "sequential_solves_per_s": ub.total / t_seq,
+           "graph_speedup": t_seq / t_graph, "plan_streams": plan.streams,
+           "achieved_fp64_tflops": flops / t_graph / 1e12, "failed_matrices": bad,
+           "regimes": {str(n): ub.solvers[n].regime for n in ub.counts}}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.serving:
         run_serving(args)
+    elif args.uneven:
+        run_uneven(args)
     else:
         run_ours(args)
 

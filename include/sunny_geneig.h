@@ -94,7 +94,9 @@ void sunny_geneig_destroy(sunny_geneig_solver_t solver);
  * LAUNCH_ERROR when the CUDA launch itself fails. One handle may be used
  * from several streams: for sizes whose solver keeps scratch slots (the
  * "l2-slot" regime) a launch on a different stream than the previous one
- * waits for it on the device, so launches of one such handle never overlap. */
+ * waits for it on the device, so launches of one such handle never overlap
+ * (while a stream is being captured into a CUDA graph this ordering is left
+ * to the graph: capture each such handle's launches on one stream). */
 sunny_geneig_status_t sunny_geneig_launch(
     sunny_geneig_solver_t solver,
     uintptr_t             d_H,

@@ -1,0 +1,249 @@
+"""Uneven-size batches: many problems whose N varies, solved by one graph launch.
+
+Problems are grouped by N into packed, batch-contiguous buffers (one group
+per size, the C-ABI layout). Each size class gets its own solver handle and
+its own CUDA stream; all classes are launched concurrently and the whole set
+of launches is captured once into a CUDA graph, so that a batch of the same
+shape is re-run by a single graph launch (`UnevenBatch.replay`). The plain
+alternative (`run_sequential`) is one launch per size on one stream.
+
+The launch plan (how many streams, which sizes share a stream, in which
+order) is picked by `autotune`: it times every size class alone, spreads the
+classes over k streams by longest-processing-time-first for each candidate
+k, captures and times each candidate graph, and keeps the fastest. Choices
+are remembered per size mix in an on-disk table (`TuneTable`), written
+atomically (temporary file + rename) and validated when read; a corrupt or
+foreign file is ignored and rewritten.
+"""
+from __future__ import annotations
+
+import json
+import os
+import tempfile
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Dict, List, Optional, Sequence
+
+TABLE_VERSION = 1
+
+
+def default_table_path() -> Path:
+    env = os.environ.get("SUNNY_GENEIG_TUNE_TABLE")
+    if env:
+        return Path(env)
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return Path(base) / "sunny_geneig" / "uneven_plans.json"
+
+
+def mix_key(counts: Dict[int, int], device_name: str = "") -> str:
+    """Key of a size mix: sizes with counts rounded to 2 significant figures."""
+    def r2(c):
+        s = f"{c:.2g}"
+        return str(int(float(s)))
+    return device_name + "|" + ",".join(f"{n}:{r2(c)}" for n, c in sorted(counts.items()))
+
+
+@dataclass
+class Plan:
+    streams: List[List[int]]      # sizes launched on each stream, in order
+
+    def to_json(self):
+        return {"streams": self.streams}
+
+    @staticmethod
+    def from_json(d) -> "Plan":
+        if not isinstance(d, dict) or not isinstance(d.get("streams"), list):
+            raise ValueError("bad plan")
+        st = []
+        for lane in d["streams"]:
+            if not isinstance(lane, list) or not all(isinstance(x, int) and x > 0 for x in lane):
+                raise ValueError("bad plan lane")
+            st.append(list(lane))
+        if not st:
+            raise ValueError("empty plan")
+        return Plan(st)
+
+
+class TuneTable:
+    """Persisted {size mix -> Plan}; atomic writes, validated reads."""
+
+    def __init__(self, path: Optional[Path] = None, enabled: bool = True):
+        self.path = Path(path) if path else default_table_path()
+        self.enabled = enabled
+        self.plans: Dict[str, Plan] = {}
+        self.rejected = False
+        if enabled:
+            self._load()
+
+    def _load(self):
+        try:
+            raw = json.loads(self.path.read_text())
+        except FileNotFoundError:
+            return
+        except (OSError, ValueError):
+            self.rejected = True
+            return
+        try:
+            if raw.get("format") != "sunny-geneig-uneven-plans" or raw.get("version") != TABLE_VERSION:
+                raise ValueError("foreign table")
+            self.plans = {str(k): Plan.from_json(v) for k, v in raw["plans"].items()}
+        except (AttributeError, KeyError, TypeError, ValueError):
+            self.plans = {}
+            self.rejected = True
+
+    def get(self, key: str) -> Optional[Plan]:
+        return self.plans.get(key)
+
+    def put(self, key: str, plan: Plan) -> None:
+        self.plans[key] = plan
+        if not self.enabled:
+            return
+        self.path.parent.mkdir(parents=True, exist_ok=True)
+        body = {"format": "sunny-geneig-uneven-plans", "version": TABLE_VERSION,
+                "plans": {k: p.to_json() for k, p in self.plans.items()}}
+        fd, tmp = tempfile.mkstemp(prefix=".plans.", dir=str(self.path.parent))
+        try:
+            with os.fdopen(fd, "w") as f:
+                json.dump(body, f)
+            os.replace(tmp, self.path)
+        except BaseException:
+            try:
+                os.unlink(tmp)
+            except OSError:
+                pass
+            raise
+
+
+def lpt_plan(cost: Dict[int, float], k: int) -> Plan:
+    """Longest-processing-time-first assignment of size classes to k streams."""
+    lanes = [[] for _ in range(max(1, min(k, len(cost))))]
+    load = [0.0] * len(lanes)
+    for n in sorted(cost, key=lambda x: -cost[x]):
+        j = min(range(len(lanes)), key=lambda t: load[t])
+        lanes[j].append(n)
+        load[j] += cost[n]
+    return Plan([l for l in lanes if l])
+
+
+class UnevenBatch:
+    """Device buffers and launches for a batch of problems of varying N.
+
+    `sizes[p]` is the size of problem p; `set_inputs(n, H, S)` fills the
+    column-major buffers of size class n (tensors of shape (count_n, n, n))."""
+
+    def __init__(self, sizes: Sequence[int], device=None):
+        import torch
+        from .solver import Solver
+        self.torch = torch
+        self.dev = torch.device(device if device is not None else "cuda")
+        counts: Dict[int, int] = {}
+        for n in sizes:
+            counts[int(n)] = counts.get(int(n), 0) + 1
+        self.counts = dict(sorted(counts.items()))
+        self.H, self.S, self.W, self.U, self.info = {}, {}, {}, {}, {}
+        self.solvers, self.streams = {}, {}
+        for n, c in self.counts.items():
+            self.H[n] = torch.empty((c, n, n), dtype=torch.complex128, device=self.dev)
+            self.S[n] = torch.empty((c, n, n), dtype=torch.complex128, device=self.dev)
+            self.W[n] = torch.empty((c, n), dtype=torch.float64, device=self.dev)
+            self.U[n] = torch.empty((c, n, n), dtype=torch.complex128, device=self.dev)
+            self.info[n] = torch.empty((c,), dtype=torch.int32, device=self.dev)
+            self.solvers[n] = Solver(n, device_id=self.dev.index or 0)
+        self.graph = None
+        self.plan: Optional[Plan] = None
+
+    @property
+    def total(self) -> int:
+        return sum(self.counts.values())
+
+    def set_inputs(self, n: int, H, S) -> None:
+        self.H[n].copy_(H)
+        self.S[n].copy_(S)
+
+    def _launch(self, n, stream):
+        self.solvers[n].launch(self.H[n], self.S[n], self.W[n], self.U[n], self.info[n], stream)
+
+    def run_sequential(self, stream=None) -> None:
+        """One plain launch per size class, one after the other on one stream."""
+        s = stream or self.torch.cuda.current_stream(self.dev)
+        for n in self.counts:
+            self._launch(n, s)
+
+    def _lane_streams(self, plan: Plan):
+        torch = self.torch
+        while len(self.streams) < len(plan.streams):
+            self.streams[len(self.streams)] = torch.cuda.Stream(self.dev)
+        return [self.streams[i] for i in range(len(plan.streams))]
+
+    def capture(self, plan: Plan):
+        """Capture the launches of `plan` into one CUDA graph (each size class on
+        its plan stream: the same stream it is warmed up on, so that handles
+        with scratch slots never wait across streams)."""
+        torch = self.torch
+        lanes = self._lane_streams(plan)
+        cur = torch.cuda.current_stream(self.dev)
+        for lane, s in zip(plan.streams, lanes):      # warm-up on the capture streams
+            s.wait_stream(cur)
+            for n in lane:
+                self._launch(n, s)
+            cur.wait_stream(s)
+        torch.cuda.synchronize(self.dev)
+        g = torch.cuda.CUDAGraph()
+        root = lanes[0]
+        with torch.cuda.graph(g, stream=root):
+            for lane, s in zip(plan.streams, lanes):
+                if s is not root:
+                    s.wait_stream(root)
+                for n in lane:
+                    self._launch(n, s)
+            for s in lanes:
+                if s is not root:
+                    root.wait_stream(s)
+        self.graph, self.plan = g, plan
+        return g
+
+    def replay(self) -> None:
+        self.graph.replay()
+
+    def _time(self, fn, reps: int = 3) -> float:
+        torch = self.torch
+        fn()
+        torch.cuda.synchronize(self.dev)
+        best = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) * 1e-3)
+        return best
+
+    def autotune(self, table: Optional[TuneTable] = None, candidates=(1, 2, 3, 4, 8)) -> Plan:
+        """Pick and capture the fastest plan (see module docstring)."""
+        torch = self.torch
+        name = torch.cuda.get_device_name(self.dev)
+        key = mix_key(self.counts, name)
+        if table is not None:
+            known = table.get(key)
+            if known is not None and sorted(x for l in known.streams for x in l) == sorted(self.counts):
+                self.capture(known)
+                return known
+        cur = torch.cuda.current_stream(self.dev)
+        cost = {n: self._time(lambda n=n: self._launch(n, cur), reps=1) for n in self.counts}
+        best, best_t = None, float("inf")
+        seen = set()
+        for k in candidates:
+            plan = lpt_plan(cost, k)
+            sig = json.dumps(plan.streams)
+            if sig in seen:
+                continue
+            seen.add(sig)
+            self.capture(plan)
+            t = self._time(self.replay, reps=3)
+            if t < best_t:
+                best, best_t = plan, t
+        self.capture(best)
+        if table is not None:
+            table.put(key, best)
+        return best

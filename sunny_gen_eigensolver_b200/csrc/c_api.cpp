@@ -148,6 +148,9 @@ sunny_geneig_status_t launch_impl(sunny_geneig_solver_t s, int stage, uintptr_t 
             std::lock_guard<std::mutex> lock(s->scratch_mu);
             e = with_device(s->device, [&]() {
                 const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+                    return run();   // inside a capture the graph's dependencies order the launches
                 if (s->scratch_used && s->last_stream != stream) {
                     cudaError_t w = cudaStreamWaitEvent(st, s->scratch_done, 0);
                     if (w != cudaSuccess) return w;
