@@ -23,6 +23,11 @@
 //
 // Output: Z (n x n, column slot j holds the eigenvector of w[j]); w[] in the
 // caller's units. Eigenvalues are not sorted here.
+//
+// NMAX > 0 bounds n at compile time (Z, U in shared memory; merge products
+// accumulate in registers). NMAX == 0 is the any-n form for matrices kept in
+// global memory: merges wider than 32 columns are 16 x 16 FP64 tensor-core
+// tiles written to the separate buffer Zo and copied back.
 #pragma once
 
 #include "geneig_common.cuh"
@@ -32,6 +37,7 @@ namespace sgeig {
 struct DCShared {
     double* Z;  int ldz;    // eigenvectors
     double* U;  int ldu;    // K x K blocks of each merge at [a, a+K)^2
+    double* Zo;             // NMAX == 0 only: n x ldz product buffer of the merge GEMMs
     double* d;  double* e;  // tridiagonal (modified)
     double* w;              // eigenvalue of column slot j
     double* z;              // merge z-vector by column slot
@@ -183,6 +189,144 @@ __host__ __device__ inline int secular_root_p(int i, int K, const double* dl, co
 __host__ __device__ inline int secular_root(int i, int K, const double* dl, const double* zz, double rho,
                                             double& tau_out, int& org_out) {
     return secular_root_p<1>(i, K, dl, zz, rho, 0, 0u, tau_out, org_out);
+}
+
+// Phase E of a level whose single merge covers [0, n): 8x8 output tiles on
+// the FP64 tensor cores (mma.m8n8k4.f64), one warp per tile, accumulators in
+// registers (n <= NMAX); all reads finish before the barrier, then the tiles
+// are written back to the gathered columns.
+template <int NT, int NMAX>
+__device__ __forceinline__ void dc_merge_top_regs(int n, const DCShared& s) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    const int K = s.kcnt[0];
+    const int tm = (n + 7) >> 3, tn = (K + 7) >> 3;
+    constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + NW - 1) / NW;
+    double acc[MAXT][2];
+#pragma unroll
+    for (int u = 0; u < MAXT; ++u) {
+        acc[u][0] = acc[u][1] = 0.0;
+        const int t = warp + NW * u;
+        if (K == 0 || t >= tm * tn) continue;
+        const int ti = t / tn, tj = t - ti * tn;
+        const int ia = 8 * ti + (lane >> 2), jb = 8 * tj + (lane >> 2);
+        for (int k = 0; k < K; k += 4) {
+            const int ka = k + (lane & 3);
+            const double av = (ia < n && ka < K) ? s.Z[ia + (size_t)s.nd[ka] * s.ldz] : 0.0;
+            const double bv = (ka < K && jb < K) ? s.U[ka + (size_t)jb * s.ldu] : 0.0;
+            asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                : "+d"(acc[u][0]), "+d"(acc[u][1]) : "d"(av), "d"(bv));
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < MAXT; ++u) {
+        const int t = warp + NW * u;
+        if (K == 0 || t >= tm * tn) continue;
+        const int ti = t / tn, tj = t - ti * tn;
+        const int r = 8 * ti + (lane >> 2), j = 8 * tj + 2 * (lane & 3);
+        if (r < n && j < K) s.Z[r + (size_t)s.nd[j] * s.ldz] = acc[u][0];
+        if (r < n && j + 1 < K) s.Z[r + (size_t)s.nd[j + 1] * s.ldz] = acc[u][1];
+    }
+}
+
+// Phase E of a level of merges at most 4 * UMAX columns wide: four lanes per
+// row, lane q accumulating output columns j = q + 4u in registers. A row's
+// reads and writes stay within its quad, so no barrier is needed between them.
+template <int NT, int UMAX>
+__device__ __forceinline__ void dc_merge_rows_regs(int n, int half, int span, const DCShared& s) {
+    for (int p0 = 0; p0 < 4 * n; p0 += NT) {
+        const int pidx = p0 + threadIdx.x;
+        const int r = pidx >> 2, part = pidx & 3;
+        const int a = (r < n) ? r - r % span : n;
+        const bool active = r < n && a + half < n && s.kcnt[a] > 0;
+        const int K = active ? s.kcnt[a] : 0;
+        double acc[UMAX];
+#pragma unroll
+        for (int u = 0; u < UMAX; ++u) acc[u] = 0.0;
+        for (int l = 0; l < K; ++l) {
+            const double x = s.Z[r + (size_t)s.nd[a + l] * s.ldz];
+            const double* ur = s.U + (a + l) + (size_t)(a + part) * s.ldu;
+#pragma unroll
+            for (int u = 0; u < UMAX; ++u)
+                if (part + 4 * u < K) acc[u] = fma(x, ur[(size_t)(4 * u) * s.ldu], acc[u]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < UMAX; ++u) {
+            const int j = part + 4 * u;
+            if (j < K) s.Z[r + (size_t)s.nd[a + j] * s.ldz] = acc[u];
+        }
+    }
+}
+
+// Phase E for any merge width (NMAX == 0): for every merge [a, a+m) of the
+// level, the m x K product Z(a:a+m, nd) * U on the FP64 tensor cores in
+// 16 x 16 warp tiles (2 x 2 mma.m8n8k4 tiles), rows outside [a, a+m) being
+// zero in those columns. Tiles are dealt round-robin to the warps across all
+// merges of the level; products go to Zo, then back into Z after a barrier.
+template <int NT>
+__device__ __forceinline__ void dc_merge_tiled(int n, int half, int span, const DCShared& s) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    int dealt = 0;
+    for (int a = 0; a + half < n; a += span) {
+        const int K = s.kcnt[a];
+        if (K == 0) continue;
+        const int m = min(span, n - a);
+        const int tn = (K + 15) >> 4, T = ((m + 15) >> 4) * tn;
+        const int* nd = s.nd + a;
+        const double* Ub = s.U + a + (size_t)a * s.ldu;
+        int t = (warp - dealt % NW + NW) % NW;
+        for (; t < T; t += NW) {
+            const int ti = t / tn, tj = t - ti * tn;
+            const int r0 = 16 * ti + (lane >> 2), j0 = 16 * tj + (lane >> 2);
+            double acc[2][2][2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int g = 0; g < 2; ++g) acc[h][g][0] = acc[h][g][1] = 0.0;
+#pragma unroll 2
+            for (int k = 0; k < K; k += 4) {
+                const int ka = k + (lane & 3);
+                const bool kin = ka < K;
+                const double* zc = s.Z + a + (size_t)(kin ? nd[ka] : 0) * s.ldz;
+                double av[2], bv[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    av[h] = (kin && r0 + 8 * h < m) ? zc[r0 + 8 * h] : 0.0;
+                    bv[h] = (kin && j0 + 8 * h < K) ? Ub[ka + (size_t)(j0 + 8 * h) * s.ldu] : 0.0;
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int g = 0; g < 2; ++g)
+                        asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                            : "+d"(acc[h][g][0]), "+d"(acc[h][g][1]) : "d"(av[h]), "d"(bv[g]));
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = 16 * ti + 8 * h + (lane >> 2);
+                if (r >= m) continue;
+#pragma unroll
+                for (int g = 0; g < 2; ++g) {
+                    const int j = 16 * tj + 8 * g + 2 * (lane & 3);
+                    if (j < K) s.Zo[a + r + (size_t)nd[j] * s.ldz] = acc[h][g][0];
+                    if (j + 1 < K) s.Zo[a + r + (size_t)nd[j + 1] * s.ldz] = acc[h][g][1];
+                }
+            }
+        }
+        dealt += T;
+    }
+    __syncthreads();
+    const int width = min(span, n);
+    for (int idx = threadIdx.x; idx < n * width; idx += NT) {
+        const int jj = idx / n, r = idx - jj * n;
+        const int a = r - r % span;
+        if (a + half >= n || jj >= s.kcnt[a]) continue;
+        const size_t o = r + (size_t)s.nd[a + jj] * s.ldz;
+        s.Z[o] = s.Zo[o];
+    }
 }
 
 // All NT threads of the CTA call this. n >= 1. On return Z, w hold the
@@ -375,67 +519,12 @@ __device__ void tridiag_dc(int n, DCShared s) {
         }
         __syncthreads();
         // ---- phase E: Z(:, nd) <- Z(:, nd) * U.
-        if (span >= n) {
-            // one merge over [0, n): 8x8 output tiles on the FP64 tensor cores
-            // (mma.m8n8k4.f64), one warp per tile; all reads finish before the
-            // barrier, then the tiles are written back to the gathered columns.
-            const int K = s.kcnt[0];
-            const int tm = (n + 7) >> 3, tn = (K + 7) >> 3;
-            constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + NW - 1) / NW;
-            double acc[MAXT][2];
-#pragma unroll
-            for (int u = 0; u < MAXT; ++u) {
-                acc[u][0] = acc[u][1] = 0.0;
-                const int t = warp + NW * u;
-                if (K == 0 || t >= tm * tn) continue;
-                const int ti = t / tn, tj = t - ti * tn;
-                const int ia = 8 * ti + (lane >> 2), jb = 8 * tj + (lane >> 2);
-                for (int k = 0; k < K; k += 4) {
-                    const int ka = k + (lane & 3);
-                    const double av = (ia < n && ka < K) ? s.Z[ia + (size_t)s.nd[ka] * s.ldz] : 0.0;
-                    const double bv = (ka < K && jb < K) ? s.U[ka + (size_t)jb * s.ldu] : 0.0;
-                    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                        : "+d"(acc[u][0]), "+d"(acc[u][1]) : "d"(av), "d"(bv));
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int u = 0; u < MAXT; ++u) {
-                const int t = warp + NW * u;
-                if (K == 0 || t >= tm * tn) continue;
-                const int ti = t / tn, tj = t - ti * tn;
-                const int r = 8 * ti + (lane >> 2), j = 8 * tj + 2 * (lane & 3);
-                if (r < n && j < K) s.Z[r + (size_t)s.nd[j] * s.ldz] = acc[u][0];
-                if (r < n && j + 1 < K) s.Z[r + (size_t)s.nd[j + 1] * s.ldz] = acc[u][1];
-            }
+        if constexpr (NMAX > 0) {
+            if (span >= n) dc_merge_top_regs<NT, NMAX>(n, s);
+            else dc_merge_rows_regs<NT, pow2_below(NMAX) / 4>(n, half, span, s);
         } else {
-            // several merges, each of at most `span` columns, span being at most
-            // the largest power of two below NMAX: four lanes per row, lane q
-            // accumulating output columns j = q + 4u in registers
-            constexpr int UMAX = pow2_below(NMAX) / 4;
-            for (int p0 = 0; p0 < 4 * n; p0 += NT) {
-                const int pidx = p0 + tid;
-                const int r = pidx >> 2, part = pidx & 3;
-                const int a = (r < n) ? r - r % span : n;
-                const bool active = r < n && a + half < n && s.kcnt[a] > 0;
-                const int K = active ? s.kcnt[a] : 0;
-                double acc[UMAX];
-#pragma unroll
-                for (int u = 0; u < UMAX; ++u) acc[u] = 0.0;
-                for (int l = 0; l < K; ++l) {
-                    const double x = s.Z[r + (size_t)s.nd[a + l] * s.ldz];
-                    const double* ur = s.U + (a + l) + (size_t)(a + part) * s.ldu;
-#pragma unroll
-                    for (int u = 0; u < UMAX; ++u)
-                        if (part + 4 * u < K) acc[u] = fma(x, ur[(size_t)(4 * u) * s.ldu], acc[u]);
-                }
-                __syncwarp();
-#pragma unroll
-                for (int u = 0; u < UMAX; ++u) {
-                    const int j = part + 4 * u;
-                    if (j < K) s.Z[r + (size_t)s.nd[a + j] * s.ldz] = acc[u];
-                }
-            }
+            if (span <= 32) dc_merge_rows_regs<NT, 8>(n, half, span, s);
+            else dc_merge_tiled<NT>(n, half, span, s);
         }
         __syncthreads();
     }

@@ -5,17 +5,19 @@
 //   a2  A <- L, S = L L^H (lower Cholesky)        (:244)
 //   a3  B <- L^-1 H                               (:246)
 //   a4  B <- B L^-H = C   (done as L^-1 (L^-1 H)^H, same value)  (:248)
-//   a5  C = Q T Q^H (Householder, lower), T = Z diag(w) Z^T by implicit QL/QR,
-//       V = Q Z                                   (:250)
+//   a5  C = Q T Q^H (Householder, lower), T = Z diag(w) Z^T by divide and
+//       conquer, V = Q Z                          (:250)
 //   a6  U = L^-H V                                (:252)
 //   a7  store W (ascending) and U                 (:268-276)
 // Column work (a3, a4, a6 and the back-transform of a5) is owned by groups
 // of G = 4 lanes per column, which synchronise with warp shuffles only; the
 // Cholesky and Householder steps use CTA barriers.
 //
-// Regimes: SmemCta keeps A and B (each n x ld complex, ld odd so that row
-// walks are bank-conflict free) in dynamic shared memory; L2Slot keeps them
-// in a per-CTA global-memory slot and only the vectors in shared memory.
+// Regimes: SmemWide keeps A and B (each n x ld complex, ld odd so that row
+// walks are bank-conflict free) in dynamic shared memory; L2Slot keeps them,
+// and an n x ld real buffer for the divide-and-conquer merge products, in a
+// per-CTA global-memory slot (l2slot_bytes) and only the vectors in shared
+// memory. L2Slot forms V = Q Z and U = L^-H V in place in the output U.
 
 #include "geneig_common.cuh"
 #include "geneig_dc.cuh"
@@ -52,8 +54,6 @@ struct VecArea {
     double*  d;     // n   tridiagonal diagonal / eigenvalues
     double*  e;     // n   tridiagonal off-diagonal
     double*  rdg;   // n   1 / L_kk
-    double*  rc;    // n   rotation cosines of the current sweep
-    double*  rs;    // n   rotation sines of the current sweep
     int*     rank;  // n   ascending position of eigenvalue j
     int*     ctl;   // 8   control words
     double*  dcd;   // divide-and-conquer doubles (dc_vec_doubles(n))
@@ -61,7 +61,7 @@ struct VecArea {
 };
 
 __host__ __device__ inline size_t vec_area_bytes(int n) {
-    return (size_t)n * 16 * 3 + 32 * 16 + (size_t)n * 8 * 5 + (size_t)n * 4 + 8 * 4 +
+    return (size_t)n * 16 * 3 + 32 * 16 + (size_t)n * 8 * 3 + (size_t)n * 4 + 8 * 4 +
            (size_t)dc_vec_doubles(n) * 8 + (size_t)dc_vec_ints(n) * 4;
 }
 
@@ -74,14 +74,20 @@ __device__ inline VecArea carve(unsigned char* p, int n) {
     v.d   = reinterpret_cast<double*>(v.red + 32);
     v.e   = v.d + n;
     v.rdg = v.e + n;
-    v.rc  = v.rdg + n;
-    v.rs  = v.rc + n;
-    v.dcd  = v.rs + n;
+    v.dcd  = v.rdg + n;
     v.rank = reinterpret_cast<int*>(v.dcd + dc_vec_doubles(n));
     v.ctl  = v.rank + n;
     v.dci  = v.ctl + 8;
     return v;
 }
+
+// Per-CTA scratch slot of the L2Slot regime, in double2 units: A, B (n x ld
+// complex each) and the n x ld real merge-product buffer.
+__host__ __device__ inline size_t l2slot_elems(int n) {
+    const size_t mat = (size_t)n * (n | 1);
+    return 2 * mat + (mat + 1) / 2;
+}
+__host__ __device__ inline size_t l2slot_bytes(int n) { return l2slot_elems(n) * 16; }
 
 // X <- L^-1 X for the columns of X owned by this group (rows split by lane).
 __device__ __forceinline__ void group_forward_solve(const double2* A, const double* rdg, double2* X,
@@ -108,10 +114,12 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
 
     double2* A;
     double2* B;
+    double* Zo = nullptr;
     unsigned char* vec_base;
     if (kL2Slot) {
-        A = a.scratch + (size_t)blockIdx.x * 2 * mat;
+        A = a.scratch + (size_t)blockIdx.x * l2slot_elems(n);
         B = A + mat;
+        Zo = reinterpret_cast<double*>(B + mat);
         vec_base = smem_raw;
     } else {
         A = reinterpret_cast<double2*>(smem_raw);
@@ -277,12 +285,13 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
                 if (n == 1) v.tau[0] = c2(0.0, 0.0);
             }
             __syncthreads();
-            if constexpr (!kL2Slot) {
-                // ---- a5b: divide and conquer on T; Z (real) and its merge
-                // workspace share B's storage, eigenvalues land in dcd[0..n).
+            // ---- a5b: divide and conquer on T; Z (real) and its merge
+            // workspace share B's storage, eigenvalues land in dcd[0..n).
+            {
                 DCShared dc;
                 dc.Z = reinterpret_cast<double*>(B); dc.ldz = ld;
                 dc.U = dc.Z + (size_t)n * ld;        dc.ldu = ld;
+                dc.Zo = Zo;
                 dc.d = v.d; dc.e = v.e;
                 dc.w = v.dcd; dc.z = dc.w + n; dc.dl = dc.z + n; dc.zz = dc.dl + n; dc.zh = dc.zz + n;
                 dc.rt = dc.zh + n; dc.rho = dc.rt + n; dc.scal = dc.rho + n;
@@ -295,32 +304,6 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
                 }
                 __syncthreads();
                 if (v.ctl[4]) code = v.ctl[4];
-            } else {
-                // ---- a5b: Z = I (kept in the real parts of B), implicit QL/QR.
-                for (int idx = tid; idx < (int)nn; idx += kNT) {
-                    const int j = idx / n, i = idx - j * n;
-                    B[i + (size_t)j * ld] = c2(i == j ? 1.0 : 0.0, 0.0);
-                }
-                TridiagQL ql;
-                if (tid == 0) ql.init(n);
-                __syncthreads();
-                for (;;) {
-                    if (tid == 0) {
-                        int lo = 0; bool backward = true;
-                        const int cnt = ql.next(v.d, v.e, v.rc, v.rs, lo, backward);
-                        v.ctl[1] = cnt; v.ctl[2] = lo; v.ctl[3] = backward ? 1 : 0;
-                        if (cnt == 0) v.ctl[4] = ql.info;
-                    }
-                    __syncthreads();
-                    const int cnt = v.ctl[1];
-                    if (cnt == 0) break;
-                    const int lo = v.ctl[2];
-                    const bool backward = v.ctl[3] != 0;
-                    for (int i = tid; i < n; i += kNT) apply_sweep_row(B + i, ld, v.rc, v.rs, lo, cnt, backward);
-                    __syncthreads();
-                }
-                if (v.ctl[4]) code = v.ctl[4];
-                for (int i = tid; i < n; i += kNT) v.dcd[i] = v.d[i];
             }
             // ascending rank of each eigenvalue
             if (!code) {
@@ -425,9 +408,14 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
                 if (q == 0) Wb[r] = v.dcd[j];
             }
         } else {
-            // a5c + a6 + a7 in place in B, one column per group: V = Q Z, U = L^-H V.
+            // a5c + a6 + a7 in place in the output, one column per group:
+            // column rank[j] of U <- z_j, then V = Q Z, then U = L^-H V. Lane q
+            // touches only rows i = q mod G of its column throughout.
+            const double* Z = reinterpret_cast<const double*>(B);
             for (int j = g; j < n; j += NG) {
-                double2* x = B + (size_t)j * ld;
+                const int r = v.rank[j];
+                double2* x = Ub + (size_t)r * n;
+                for (int i = q; i < n; i += kG) x[i] = c2(Z[i + (size_t)j * ld], 0.0);
                 for (int k = n - 2; k >= 0; --k) {
                     const double2 tk = v.tau[k];
                     if (tk.x == 0.0 && tk.y == 0.0) continue;
@@ -453,9 +441,6 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
                         for (int k = q; k < i; k += kG) x[k] = cfmsc(x[k], A[i + (size_t)k * ld], ui);
                     }
                 }
-                const int r = v.rank[j];
-                double2* uo = Ub + (size_t)r * n;
-                for (int i = q; i < n; i += kG) uo[i] = x[i];
                 if (q == 0) Wb[r] = v.dcd[j];
             }
         }
@@ -513,7 +498,7 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
             p.regime = Regime::L2Slot;
             p.smem = vec_area_bytes(n);
             p.slots = 2 * sms;
-            p.scratch_bytes = (size_t)p.slots * 2 * n * p.ld * 16;
+            p.scratch_bytes = (size_t)p.slots * l2slot_bytes(n);
         }
         e = cudaFuncSetAttribute(kernel_for(p.regime), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     }
@@ -599,7 +584,7 @@ extern "C" sunny_geneig_status_t sunny_geneig_launch_noalloc(int n, uintptr_t d_
                                                              uintptr_t stream) {
     using namespace sgeig;
     api_clear_error();
-    const size_t slot = (n >= 1) ? (size_t)2 * n * (size_t)(n | 1) * 16 : 0;
+    const size_t slot = (n >= 1 && n <= kMaxN) ? l2slot_bytes(n) : 0;
     if (n < 1 || n > kMaxN || slot > kNoAllocScratchBytes) {
         api_set_error("sunny_geneig_launch_noalloc: n=" + std::to_string(n) + " outside [1, " +
                       std::to_string(kMaxN) + "] (the static scratch holds " +
