@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--e2e-chunk", type=int, default=8192)
+    p.add_argument("--sigma", action="store_true",
+                   help="spin-wave metric pencils: H = diag(I, -I) implied (sunny_geneig_launch_sigma), "
+                        "S = the BdG matrix")
     p.add_argument("--serving", action="store_true", help="run the serving-loop workload instead")
     p.add_argument("--uneven", action="store_true", help="run the uneven-size batch workload instead")
     p.add_argument("--uneven-total", type=int, default=200000, help="uneven: number of problems")
@@ -108,7 +111,10 @@ def run_reference(args):
 
 def workload_config(args, world):
     return {
-        "workload": (f"N={args.n} complex128 Hermitian-definite pairs, batch {args.batch} per GPU, "
+        "workload": (f"N={args.n} complex128 spin-wave metric pencils (diag(I, -I), S), batch {args.batch} "
+                     f"per GPU, S = BdG-structured PD matrix (lambda_min = 0.1 ||S||); H implied, not read; "
+                     f"one launch per step" if getattr(args, "sigma", False) else
+                     f"N={args.n} complex128 Hermitian-definite pairs, batch {args.batch} per GPU, "
                      f"BdG-structured H (lambda_min = 0.1 ||H||), S = Q diag(d) Q^H with cond(S) <= "
                      f"{args.kappa:g}; one launch per step"),
         "n": args.n, "batch_per_gpu": args.batch, "global_batch": args.batch * world,
@@ -206,6 +212,10 @@ def run_ours(args):
     n, batch = args.n, args.batch
     H, S = baseline_problems_torch(n, batch, seed=replicas.rank_seed(20261203 + 1, rank), kappa=args.kappa,
                                    device=dev)
+    if args.sigma:
+        # Sunny's pattern: the PD BdG matrix is the metric-side S, H = diag(I, -I)
+        sig = torch.cat([torch.ones(n // 2), -torch.ones(n - n // 2)]).to(torch.complex128)
+        S, H = H, torch.diag(sig).to(dev).expand(batch, n, n)
     H = H.transpose(-1, -2).contiguous()   # column-major buffers (Julia layout)
     S = S.transpose(-1, -2).contiguous()
     W = torch.empty((batch, n), dtype=torch.float64, device=dev)
@@ -219,8 +229,14 @@ def run_ours(args):
     def barrier():
         replicas.barrier(dev)
 
+    def do_launch(Hx, Sx, Wx, Ux, ix, st):
+        if args.sigma:
+            solver.launch_sigma(Sx, Wx, Ux, ix, st)
+        else:
+            solver.launch(Hx, Sx, Wx, Ux, ix, st)
+
     for _ in range(args.warmup):
-        solver.launch(H, S, W, U, info, stream)
+        do_launch(H, S, W, U, info, stream)
     barrier()
     props = torch.cuda.get_device_properties(dev)
     uuid = getattr(props, "uuid", None)
@@ -230,7 +246,7 @@ def run_ours(args):
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         for _ in range(args.steps):
-            solver.launch(H, S, W, U, info, stream)
+            do_launch(H, S, W, U, info, stream)
         t1.record(stream)
         barrier()
     elapsed = t0.elapsed_time(t1) * 1e-3
@@ -260,7 +276,7 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": hbm_bytes_per_solve(n) * batch,
                 "achieved_hbm_gbs": hbm_bytes_per_solve(n) * batch / per_launch / 1e9}
     tfile = REPO / "profiles" / f"dram_traffic_n{n}.json"
-    if tfile.exists():
+    if tfile.exists() and not args.sigma:
         try:
             t = json.loads(tfile.read_text())
             roofline["traffic"] = t["dram_bytes_per_solve"] * batch
@@ -270,7 +286,7 @@ def run_ours(args):
 
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, torch, solver, H, S, W, U, info, dev, world, dist)
+        e2e = run_e2e(args, torch, do_launch, H, S, W, U, info, dev, world, dist)
 
     if rank == 0:
         out = {
@@ -290,12 +306,13 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_e2e(args, torch, solver, H, S, W, U, info, dev, world, dist):
+def run_e2e(args, torch, do_launch, H, S, W, U, info, dev, world, dist):
     """Same metric through the C ABI with HOST buffers: every step copies H and
-    S in from pinned host memory and W, U, info back out, pipelined in chunks
-    over three streams (H2D, launch and D2H of different chunks overlap)."""
+    S (S alone for the metric solve) in from pinned host memory and W, U, info
+    back out, pipelined in chunks over three streams (H2D, launch and D2H of
+    different chunks overlap)."""
     batch, n = args.batch, args.n
-    Hh = H.cpu().pin_memory()
+    Hh = H.cpu().pin_memory() if not args.sigma else None
     Sh = S.cpu().pin_memory()
     Wh = torch.empty(W.shape, dtype=W.dtype).pin_memory()
     Uh = torch.empty(U.shape, dtype=U.dtype).pin_memory()
@@ -308,9 +325,10 @@ def run_e2e(args, torch, solver, H, S, W, U, info, dev, world, dist):
             sl = slice(off, min(batch, off + chunk))
             s = streams[k % len(streams)]
             with torch.cuda.stream(s):
-                H[sl].copy_(Hh[sl], non_blocking=True)
+                if Hh is not None:
+                    H[sl].copy_(Hh[sl], non_blocking=True)
                 S[sl].copy_(Sh[sl], non_blocking=True)
-                solver.launch(H[sl], S[sl], W[sl], U[sl], info[sl], s)
+                do_launch(H[sl], S[sl], W[sl], U[sl], info[sl], s)
                 Wh[sl].copy_(W[sl], non_blocking=True)
                 Uh[sl].copy_(U[sl], non_blocking=True)
                 ih[sl].copy_(info[sl], non_blocking=True)
@@ -339,7 +357,7 @@ def run_e2e(args, torch, solver, H, S, W, U, info, dev, world, dist):
     if world > 1:
         dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
     el = float(el_t.item())
-    bi = 2 * batch * n * n * 16
+    bi = (1 if args.sigma else 2) * batch * n * n * 16
     bo = batch * (n * n * 16 + n * 8 + 4)
     return {"value": batch * world * steps / el, "unit": "solves/s", "h2d_bytes_per_step": bi,
             "d2h_bytes_per_step": bo, "steps": steps, "chunk": chunk, "streams": len(streams),

@@ -145,6 +145,23 @@ sunny_geneig_status_t sunny_geneig_launch_stage(
     int                   batch_size,
     uintptr_t             stream);
 
+/* Spin-wave metric solve (no counterpart in the reference's C ABI): the
+ * batch of pencils (Sigma, S) with Sigma = diag(I_{n/2}, -I_{n/2}), the
+ * para-unitary metric of linear spin-wave theory, where S is the dynamical
+ * matrix (Hermitian positive definite). Sunny calls its generalized solver in
+ * this pattern (Sigma u = lambda S u). H is implied and never read, so one
+ * matrix per problem less crosses HBM and the step T = H X^H of the
+ * reduction becomes a sign flip. n must be even. Same W/U/info layouts,
+ * info codes and error behaviour as sunny_geneig_launch. */
+sunny_geneig_status_t sunny_geneig_launch_sigma(
+    sunny_geneig_solver_t solver,
+    uintptr_t             d_S,
+    uintptr_t             d_W,
+    uintptr_t             d_U,
+    uintptr_t             d_info,
+    int                   batch_size,
+    uintptr_t             stream);
+
 /* Largest N this build accepts in sunny_geneig_create. */
 int sunny_geneig_max_matrix_size(void);
 

@@ -122,12 +122,17 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
 
 sunny_geneig_status_t launch_impl(sunny_geneig_solver_t s, int stage, uintptr_t d_H, uintptr_t d_S,
                                   uintptr_t d_W, uintptr_t d_U, uintptr_t d_info, int batch,
-                                  uintptr_t stream, const char* fn) {
+                                  uintptr_t stream, const char* fn, bool sigma = false) {
     clear_error();
     if (!s) { set_error(std::string(fn) + ": solver is NULL"); return SUNNY_GENEIG_INVALID_ARG; }
     if (batch < 0) { set_error(std::string(fn) + ": batch_size < 0"); return SUNNY_GENEIG_INVALID_ARG; }
     if (stage < 1 || stage > 4) { set_error(std::string(fn) + ": stage must be 1..4"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (sigma && (s->n & 1)) {
+        set_error(std::string(fn) + ": n must be even for the metric diag(I, -I)");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
     if (batch == 0) return SUNNY_GENEIG_OK;
+    if (sigma) d_H = d_S;   // never read; stands in for the checks below
     if (!d_H || !d_S || !d_W || !d_U || !d_info) {
         set_error(std::string(fn) + ": NULL device buffer");
         return SUNNY_GENEIG_INVALID_ARG;
@@ -141,7 +146,7 @@ sunny_geneig_status_t launch_impl(sunny_geneig_solver_t s, int stage, uintptr_t 
             return sgeig::plain_launch(s->plan, stage, reinterpret_cast<const void*>(d_H),
                                        reinterpret_cast<const void*>(d_S), reinterpret_cast<double*>(d_W),
                                        reinterpret_cast<void*>(d_U), reinterpret_cast<int*>(d_info), batch,
-                                       s->scratch, reinterpret_cast<cudaStream_t>(stream));
+                                       s->scratch, reinterpret_cast<cudaStream_t>(stream), sigma);
         };
         cudaError_t e;
         if (s->scratch) {
@@ -242,6 +247,12 @@ sunny_geneig_status_t sunny_geneig_launch_stage(sunny_geneig_solver_t solver, in
                                                 int batch_size, uintptr_t stream) {
     return launch_impl(solver, stage, d_H, d_S, d_W, d_U, d_info, batch_size, stream,
                        "sunny_geneig_launch_stage");
+}
+
+sunny_geneig_status_t sunny_geneig_launch_sigma(sunny_geneig_solver_t solver, uintptr_t d_S, uintptr_t d_W,
+                                                uintptr_t d_U, uintptr_t d_info, int batch_size, uintptr_t stream) {
+    return launch_impl(solver, 4, 0, d_S, d_W, d_U, d_info, batch_size, stream, "sunny_geneig_launch_sigma",
+                       true);
 }
 
 int sunny_geneig_matrix_size(sunny_geneig_solver_t solver) { return solver ? solver->n : -1; }

@@ -39,6 +39,7 @@ struct CtaArgs {
     int*     info;
     long long batch;
     int n, ld, stage;
+    int sigma;      // H = diag(I_{n/2}, -I_{n/2}), not read from memory
 };
 
 struct CtaVec {
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         for (int j = tr; j < n; j += 16)
             for (int i = tc; i < n; i += 16) {
                 A[i + (size_t)j * ld] = __ldg(Sb + i + (size_t)j * n);
-                B[i + (size_t)j * ld] = __ldg(Hb + i + (size_t)j * n);
+                if (!a.sigma) B[i + (size_t)j * ld] = __ldg(Hb + i + (size_t)j * n);
             }
         if (tid < 8) v.ctl[tid] = 0;
 
@@ -268,7 +269,16 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             // FP64 tensor-core tiles; T overwrites H after the barrier.
             constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + kNT / 32 - 1) / (kNT / 32);
             const int tn8 = (n + 7) >> 3;
-            {
+            if (a.sigma) {
+                // H = diag(I, -I): T(i, j) = sigma_i conj(X(j, i)), no product needed
+                const int m = n >> 1;
+                for (int j = tr; j < n; j += 16)
+                    for (int i = tc; i < n; i += 16) {
+                        const double2 x = (i <= j) ? cconj(A[j + (size_t)i * ld]) : c2(0.0, 0.0);
+                        B[i + (size_t)j * ld] = (i < m) ? x : c2(-x.x, -x.y);
+                    }
+                __syncthreads();
+            } else {
                 ZTiles<MAXT> acc;
                 ztiles_compute<MAXT>(acc, tn8, tn8,
                     [&](int i, int k) { return (i < n && k < n) ? B[i + (size_t)k * ld] : c2(0.0, 0.0); },
@@ -560,7 +570,7 @@ cudaError_t cta_set_attributes(int nmax, size_t smem) {
 }
 
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
-                       int* info, long long batch, cudaStream_t stream) {
+                       int* info, long long batch, cudaStream_t stream, bool sigma) {
     CtaArgs a;
     a.H = static_cast<const double2*>(H);
     a.S = static_cast<const double2*>(S);
@@ -571,6 +581,7 @@ cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, c
     a.n = n;
     a.ld = n | 1;
     a.stage = stage;
+    a.sigma = sigma ? 1 : 0;
     const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
     cta_kernel_for(nmax)<<<(unsigned)grid, kNT, smem, stream>>>(a);
     return cudaGetLastError();

@@ -359,6 +359,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
         if (i < n - 1) di -= fabs(s.e[i] * sc);
         s.w[i] = di;
     }
+    __syncthreads();   // every unscaled e[] read above before it is scaled in place
     for (int i = tid; i < n - 1; i += NT) s.e[i] *= sc;
     for (int idx = tid; idx < n * n; idx += NT) {
         const int j = idx / n, i = idx - j * n;

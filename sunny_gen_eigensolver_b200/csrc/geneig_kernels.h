@@ -25,8 +25,23 @@ constexpr int kCtaMaxN = 64;
 size_t cta_smem_bytes(int n);
 int cta_nmax_for(int n);
 cudaError_t cta_set_attributes(int nmax, size_t smem);
+// `sigma`: H is the metric diag(I_{n/2}, -I_{n/2}) and is not read (H may be NULL).
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
-                       int* info, long long batch, cudaStream_t stream);
+                       int* info, long long batch, cudaStream_t stream, bool sigma = false);
+
+// Tiled kernel for the L2Slot regime (geneig_tiled.cu). A CTA's slot holds
+// three n x ld complex matrices and one real one (at least 16 n complex), in
+// double2 units:
+__host__ __device__ inline size_t tiled_slot_elems(int n) {
+    const size_t mat = (size_t)n * (size_t)(n | 1);
+    const size_t zo = (mat + 1) / 2 > (size_t)16 * n ? (mat + 1) / 2 : (size_t)16 * n;
+    return 3 * mat + zo;
+}
+__host__ __device__ inline size_t tiled_slot_bytes(int n) { return tiled_slot_elems(n) * 16; }
+size_t tiled_vec_bytes(int n);
+cudaError_t tiled_set_attributes(size_t smem);
+cudaError_t tiled_launch(int n, int slots, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
+                         int* info, long long batch, void* scratch, cudaStream_t stream, bool sigma);
 
 struct PlainPlan {
     int    n        = 0;
@@ -45,10 +60,11 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err);
 
 // Enqueues one launch of `stage` (1..4) over `batch` matrices on `stream`.
 // `scratch` must hold plan.scratch_bytes when plan.regime == L2Slot.
+// `sigma`: H is diag(I_{n/2}, -I_{n/2}) (n even) and is not read.
 cudaError_t plain_launch(const PlainPlan& plan, int stage,
                          const void* H, const void* S, double* W, void* U,
                          int* info, long long batch, void* scratch,
-                         cudaStream_t stream);
+                         cudaStream_t stream, bool sigma = false);
 
 // Thread-local last-error text of the C ABI (defined in c_api.cpp), for
 // entry points implemented in other translation units.

@@ -1,4 +1,6 @@
-// Plain FP64 batched generalized Hermitian-definite eigensolver for sm_100a.
+// FP64 batched generalized Hermitian-definite eigensolver for sm_100a, the
+// "smem-wide" regime (N too large for the register-resident smem-cta kernel,
+// small enough for both working matrices to fit one CTA's shared memory).
 //
 // One CTA solves one matrix pair at a time (persistent over the batch):
 //   a1  load S -> A, H^H -> B                     (kernel_source.hpp:233-242)
@@ -11,13 +13,11 @@
 //   a7  store W (ascending) and U                 (:268-276)
 // Column work (a3, a4, a6 and the back-transform of a5) is owned by groups
 // of G = 4 lanes per column, which synchronise with warp shuffles only; the
-// Cholesky and Householder steps use CTA barriers.
+// Cholesky and Householder steps use CTA barriers. A and B are n x ld
+// complex, ld odd so that row walks are bank-conflict free.
 //
-// Regimes: SmemWide keeps A and B (each n x ld complex, ld odd so that row
-// walks are bank-conflict free) in dynamic shared memory; L2Slot keeps them,
-// and an n x ld real buffer for the divide-and-conquer merge products, in a
-// per-CTA global-memory slot (l2slot_bytes) and only the vectors in shared
-// memory. L2Slot forms V = Q Z and U = L^-H V in place in the output U.
+// This file also holds the regime choice (plain_plan), the launch dispatch
+// and the allocation-free entry point, which runs the tiled kernel.
 
 #include "geneig_common.cuh"
 #include "geneig_dc.cuh"
@@ -43,6 +43,7 @@ struct PlainArgs {
     double2* scratch;
     long long batch;
     int n, ld, stage;
+    int sigma;      // H = diag(I_{n/2}, -I_{n/2}), not read from memory
 };
 
 // Shared-memory vector area (after the matrices in the SmemCta regime).
@@ -81,14 +82,6 @@ __device__ inline VecArea carve(unsigned char* p, int n) {
     return v;
 }
 
-// Per-CTA scratch slot of the L2Slot regime, in double2 units: A, B (n x ld
-// complex each) and the n x ld real merge-product buffer.
-__host__ __device__ inline size_t l2slot_elems(int n) {
-    const size_t mat = (size_t)n * (n | 1);
-    return 2 * mat + (mat + 1) / 2;
-}
-__host__ __device__ inline size_t l2slot_bytes(int n) { return l2slot_elems(n) * 16; }
-
 // X <- L^-1 X for the columns of X owned by this group (rows split by lane).
 __device__ __forceinline__ void group_forward_solve(const double2* A, const double* rdg, double2* X,
                                                     int n, int ld, int g, int q, unsigned gmask) {
@@ -106,27 +99,15 @@ __device__ __forceinline__ void group_forward_solve(const double2* A, const doub
     }
 }
 
-template <bool kL2Slot, int NMAX>
-__global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_plain_kernel(PlainArgs a) {
+template <int NMAX>
+__global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = a.n, ld = a.ld;
     const size_t mat = (size_t)n * ld;
 
-    double2* A;
-    double2* B;
-    double* Zo = nullptr;
-    unsigned char* vec_base;
-    if (kL2Slot) {
-        A = a.scratch + (size_t)blockIdx.x * l2slot_elems(n);
-        B = A + mat;
-        Zo = reinterpret_cast<double*>(B + mat);
-        vec_base = smem_raw;
-    } else {
-        A = reinterpret_cast<double2*>(smem_raw);
-        B = A + mat;
-        vec_base = reinterpret_cast<unsigned char*>(B + mat);
-    }
-    VecArea v = carve(vec_base, n);
+    double2* A = reinterpret_cast<double2*>(smem_raw);
+    double2* B = A + mat;
+    VecArea v = carve(reinterpret_cast<unsigned char*>(B + mat), n);
 
     const int tid  = threadIdx.x;
     const int g    = tid / kG;
@@ -148,8 +129,12 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
         for (int idx = tid; idx < (int)nn; idx += kNT) {
             const int j = idx / n, i = idx - j * n;
             A[i + (size_t)j * ld] = __ldg(Sb + idx);
-            const double2 h = __ldg(Hb + idx);
-            B[j + (size_t)i * ld] = cconj(h);
+            if (a.sigma) {
+                B[j + (size_t)i * ld] = c2(i != j ? 0.0 : (2 * i < n ? 1.0 : -1.0), 0.0);
+            } else {
+                const double2 h = __ldg(Hb + idx);
+                B[j + (size_t)i * ld] = cconj(h);
+            }
         }
         if (tid < 8) v.ctl[tid] = 0;
         __syncthreads();
@@ -291,7 +276,7 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
                 DCShared dc;
                 dc.Z = reinterpret_cast<double*>(B); dc.ldz = ld;
                 dc.U = dc.Z + (size_t)n * ld;        dc.ldu = ld;
-                dc.Zo = Zo;
+                dc.Zo = nullptr;
                 dc.d = v.d; dc.e = v.e;
                 dc.w = v.dcd; dc.z = dc.w + n; dc.dl = dc.z + n; dc.zz = dc.dl + n; dc.zh = dc.zz + n;
                 dc.rt = dc.zh + n; dc.rho = dc.rt + n; dc.scal = dc.rho + n;
@@ -343,7 +328,7 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
             }
             continue;
         }
-        if constexpr (!kL2Slot) {
+        {
             // a5c + a6 + a7 in registers, one column per group (rows i = q + G t):
             // x = Q z_j, then L^H u = x, then store u as column rank[j].
             constexpr int R = NMAX / kG;
@@ -407,52 +392,13 @@ __global__ void __launch_bounds__(kNT, (NMAX > 0 && NMAX <= 64) ? 2 : 1) geneig_
                 }
                 if (q == 0) Wb[r] = v.dcd[j];
             }
-        } else {
-            // a5c + a6 + a7 in place in the output, one column per group:
-            // column rank[j] of U <- z_j, then V = Q Z, then U = L^-H V. Lane q
-            // touches only rows i = q mod G of its column throughout.
-            const double* Z = reinterpret_cast<const double*>(B);
-            for (int j = g; j < n; j += NG) {
-                const int r = v.rank[j];
-                double2* x = Ub + (size_t)r * n;
-                for (int i = q; i < n; i += kG) x[i] = c2(Z[i + (size_t)j * ld], 0.0);
-                for (int k = n - 2; k >= 0; --k) {
-                    const double2 tk = v.tau[k];
-                    if (tk.x == 0.0 && tk.y == 0.0) continue;
-                    const double2* vk = A + k;
-                    double2 s = c2(0.0, 0.0);
-                    for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
-                        const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
-                        s = cfmac(s, vi, x[i]);
-                    }
-                    s = group_sum2<kG>(gmask, s);
-                    const double2 ts = cmul(tk, s);
-                    for (int i = first_in_class<kG>(k + 1, q); i < n; i += kG) {
-                        const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
-                        x[i] = cfms(x[i], ts, vi);
-                    }
-                }
-                if (a.stage >= 4) {
-                    for (int i = n - 1; i >= 0; --i) {
-                        double2 ui = c2(0.0, 0.0);
-                        const int owner = i % kG;
-                        if (q == owner) { ui = cscale(x[i], v.rdg[i]); x[i] = ui; }
-                        ui = group_bcast2<kG>(gmask, ui, owner);
-                        for (int k = q; k < i; k += kG) x[k] = cfmsc(x[k], A[i + (size_t)k * ld], ui);
-                    }
-                }
-                if (q == 0) Wb[r] = v.dcd[j];
-            }
         }
     }
 }
 
 int g_smem_optin = -1;
 
-using KernelFn = void (*)(PlainArgs);
-KernelFn kernel_for(Regime r) {
-    return (r == Regime::L2Slot) ? geneig_plain_kernel<true, 0> : geneig_plain_kernel<false, 96>;
-}
+constexpr int kWideNmax = 96;
 
 }  // namespace
 
@@ -490,17 +436,19 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
         p.nmax = cta_nmax_for(n);
         e = cta_set_attributes(p.nmax, p.smem);
     } else {
-        if (smem_wide <= (size_t)optin && n <= 96) {
+        if (smem_wide <= (size_t)optin && n <= kWideNmax) {
             p.regime = Regime::SmemWide;
             p.smem = smem_wide;
-            p.nmax = 96;
+            p.nmax = kWideNmax;
+            e = cudaFuncSetAttribute(geneig_plain_kernel<kWideNmax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)p.smem);
         } else {
             p.regime = Regime::L2Slot;
-            p.smem = vec_area_bytes(n);
+            p.smem = tiled_vec_bytes(n);
             p.slots = 2 * sms;
-            p.scratch_bytes = (size_t)p.slots * l2slot_bytes(n);
+            p.scratch_bytes = (size_t)p.slots * tiled_slot_bytes(n);
+            e = tiled_set_attributes(p.smem);
         }
-        e = cudaFuncSetAttribute(kernel_for(p.regime), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     }
     if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
     *plan = p;
@@ -508,7 +456,7 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
 }
 
 cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const void* S, double* W,
-                         void* U, int* info, long long batch, void* scratch, cudaStream_t stream) {
+                         void* U, int* info, long long batch, void* scratch, cudaStream_t stream, bool sigma) {
     if (batch <= 0) return cudaSuccess;
     PlainArgs a;
     a.H = static_cast<const double2*>(H);
@@ -521,11 +469,13 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const 
     a.n = plan.n;
     a.ld = plan.ld;
     a.stage = stage;
+    a.sigma = sigma ? 1 : 0;
     if (plan.regime == Regime::SmemCta)
-        return cta_launch(plan.n, plan.nmax, plan.smem, stage, H, S, W, U, info, batch, stream);
-    long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
-    if (plan.regime == Regime::L2Slot && grid > plan.slots) grid = plan.slots;
-    kernel_for(plan.regime)<<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
+        return cta_launch(plan.n, plan.nmax, plan.smem, stage, H, S, W, U, info, batch, stream, sigma);
+    if (plan.regime == Regime::L2Slot)
+        return tiled_launch(plan.n, plan.slots, plan.smem, stage, H, S, W, U, info, batch, scratch, stream, sigma);
+    const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
+    geneig_plain_kernel<kWideNmax><<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -565,8 +515,7 @@ cudaError_t noalloc_setup(int dev, NoAllocDevice** out, std::string* err) {
         if (e != cudaSuccess) { *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return e; }
         e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return e; }
-        e = cudaFuncSetAttribute(geneig_plain_kernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)vec_area_bytes(kMaxN));
+        e = tiled_set_attributes(tiled_vec_bytes(kMaxN));
         if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return e; }
         d.scratch = ptr;
         d.ready = true;
@@ -584,7 +533,7 @@ extern "C" sunny_geneig_status_t sunny_geneig_launch_noalloc(int n, uintptr_t d_
                                                              uintptr_t stream) {
     using namespace sgeig;
     api_clear_error();
-    const size_t slot = (n >= 1 && n <= kMaxN) ? l2slot_bytes(n) : 0;
+    const size_t slot = (n >= 1 && n <= kMaxN) ? tiled_slot_bytes(n) : 0;
     if (n < 1 || n > kMaxN || slot > kNoAllocScratchBytes) {
         api_set_error("sunny_geneig_launch_noalloc: n=" + std::to_string(n) + " outside [1, " +
                       std::to_string(kMaxN) + "] (the static scratch holds " +
@@ -613,28 +562,12 @@ extern "C" sunny_geneig_status_t sunny_geneig_launch_noalloc(int n, uintptr_t d_
         api_set_error("sunny_geneig_launch_noalloc: " + err);
         return SUNNY_GENEIG_DEVICE_ERROR;
     }
-    PlainPlan p;
-    p.n = n;
-    p.ld = n | 1;
-    p.threads = kNT;
-    p.regime = Regime::L2Slot;
-    p.smem = vec_area_bytes(n);
     const long long fit = (long long)(kNoAllocScratchBytes / slot);
-    p.slots = (int)(fit < 2LL * d->sms ? fit : 2LL * d->sms);
-    PlainArgs a;
-    a.H = reinterpret_cast<const double2*>(d_H);
-    a.S = reinterpret_cast<const double2*>(d_S);
-    a.W = reinterpret_cast<double*>(d_W);
-    a.U = reinterpret_cast<double2*>(d_U);
-    a.info = reinterpret_cast<int*>(d_info);
-    a.scratch = static_cast<double2*>(d->scratch);
-    a.batch = batch_size;
-    a.n = n;
-    a.ld = p.ld;
-    a.stage = 4;
-    const long long grid = batch_size < p.slots ? batch_size : p.slots;
-    geneig_plain_kernel<true, 0><<<(unsigned)grid, kNT, p.smem, reinterpret_cast<cudaStream_t>(stream)>>>(a);
-    e = cudaGetLastError();
+    const int slots = (int)(fit < 2LL * d->sms ? fit : 2LL * d->sms);
+    e = tiled_launch(n, slots, tiled_vec_bytes(n), 4, reinterpret_cast<const void*>(d_H),
+                     reinterpret_cast<const void*>(d_S), reinterpret_cast<double*>(d_W), reinterpret_cast<void*>(d_U),
+                     reinterpret_cast<int*>(d_info), batch_size, d->scratch, reinterpret_cast<cudaStream_t>(stream),
+                     false);
     if (e != cudaSuccess) {
         api_set_error(std::string("sunny_geneig_launch_noalloc: kernel launch failed: ") + cudaGetErrorString(e));
         return SUNNY_GENEIG_LAUNCH_ERROR;

@@ -1,0 +1,619 @@
+// Tiled FP64 batched generalized Hermitian-definite eigensolver for sm_100a,
+// for matrices too large to keep in one CTA's shared memory (the "l2-slot"
+// regime). One CTA solves one pencil at a time, persistent over the batch;
+// its working matrices live in a per-CTA global-memory slot
+//     M0, M1, M2: n x ld complex,  Zo: n x ld real (at least 16 n complex)
+// and every O(n^3) step except the Householder reduction is a complex GEMM
+// on the FP64 tensor cores (mma.sync.m8n8k4.f64; a complex 8x8x4 step is four
+// real MMAs), one 16 x 16 output tile per warp at a time:
+//
+//   a1  M0 <- S (lower triangle)                      (kernel_source.hpp:233-242)
+//   a2  blocked Cholesky S = L L^H in M0: 16-column panels factored column
+//       by column, trailing lower tiles updated as C -= L_p L_p^H   (:244)
+//   a3  X = L^-1 in M1, one 16-row block at a time: R = L_rk X_kc (GEMM),
+//       X_r = L_rr^-1 (e_r - R) (one thread per column)            (:246)
+//   a4  T = H X^H in M2, C = X T in M0 (lower tiles, mirrored), so that
+//       C = L^-1 H L^-H; for the spin-wave metric H = diag(I, -I) the first
+//       product is a sign flip of X^H                              (:248)
+//   a5  C = Q T Q^H (Householder, lower; v_k kept in column k of M0 below
+//       the subdiagonal), T = Z diag(w) Z^T by divide and conquer (Z and its
+//       merge workspace in M2, merge products through Zo), V = Q Z with
+//       compact-WY blocks of 16 reflectors, Q_b = I - Y T_b Y^H:
+//       W1 = Y^H V, W2 = T_b W1, V -= Y W2 (all GEMMs), V in the output U   (:250)
+//   a6  U = X^H V into M2, copied to the output                   (:252)
+//   a7  W ascending, U columns in the same order                  (:268-276)
+//
+// Stage-wise outputs (stage 1: L, 2: C, 3: W and V) follow the reference's
+// static kernels in src/geneig_fixed.cu.
+
+#include "geneig_common.cuh"
+#include "geneig_dc.cuh"
+#include "geneig_kernels.h"
+#include "sunny_geneig.h"
+
+namespace sgeig {
+namespace {
+
+constexpr int kNT = 256;          // threads per CTA
+constexpr int kNW = kNT / 32;     // warps per CTA
+
+struct TiledArgs {
+    const double2* __restrict__ H;
+    const double2* __restrict__ S;
+    double*  W;
+    double2* U;
+    int*     info;
+    double2* scratch;
+    long long batch;
+    int n, ld, stage;
+    int sigma;      // H = diag(I_{n/2}, -I_{n/2}), not read from memory
+};
+
+// Shared-memory vectors of one CTA.
+struct TVec {
+    double2* tau;   // n    Householder scalars
+    double2* vb;    // n    current Householder vector (v[k+1] = 1)
+    double2* pb;    // n    tau * A22 * v
+    double2* red;   // 32   reduction scratch
+    double2* tb;    // 256  T factor of the current WY block (16 x 16, column-major)
+    double2* gb;    // 512  Y^H Y of the current WY block: two partial sums, then their sum
+    double*  d;     // n    tridiagonal diagonal
+    double*  e;     // n    tridiagonal off-diagonal
+    double*  rdg;   // n    1 / L_kk
+    double*  dcd;   // divide-and-conquer doubles (dc_vec_doubles(n)); eigenvalues first
+    int*     rank;  // n    ascending position of eigenvalue j
+    int*     ctl;   // 8    control words
+    int*     dci;   // divide-and-conquer ints (dc_vec_ints(n))
+};
+
+__device__ inline TVec tcarve(unsigned char* p, int n) {
+    TVec v;
+    v.tau = reinterpret_cast<double2*>(p);
+    v.vb  = v.tau + n;
+    v.pb  = v.vb + n;
+    v.red = v.pb + n;
+    v.tb  = v.red + 32;
+    v.gb  = v.tb + 256;
+    v.d   = reinterpret_cast<double*>(v.gb + 512);
+    v.e   = v.d + n;
+    v.rdg = v.e + n;
+    v.dcd = v.rdg + n;
+    v.rank = reinterpret_cast<int*>(v.dcd + dc_vec_doubles(n));
+    v.ctl  = v.rank + n;
+    v.dci  = v.ctl + 8;
+    return v;
+}
+
+__device__ __forceinline__ double2 cneg(double2 a) { return c2(-a.x, -a.y); }
+
+// ---------------------------------------------------------------- 16x16 complex MMA tiles
+// D(8x8) += A(8x4) B(4x8) in FP64 on the tensor cores. Fragments: lane l
+// holds A(l/4, l%4), B(l%4, l/4) and D(l/4, 2(l%4) + {0, 1}).
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
+}
+
+// A warp's 16 x 16 complex accumulator: 2 x 2 subtiles of 8 x 8, real and
+// imaginary parts apart. Element [h][g][e] is row i0 + 8h + lane/4, column
+// j0 + 8g + 2(lane%4) + e.
+struct Z16 {
+    double re[2][2][2];
+    double im[2][2][2];
+};
+
+__device__ __forceinline__ void z16_zero(Z16& c) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int g = 0; g < 2; ++g)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) c.re[h][g][e] = c.im[h][g][e] = 0.0;
+}
+
+// f(i, j) -> double2 for every element of the tile at (i0, j0)
+template <class F>
+__device__ __forceinline__ void z16_load(Z16& c, int i0, int j0, F f) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int g = 0; g < 2; ++g)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const double2 x = f(i0 + 8 * h + (lane >> 2), j0 + 8 * g + 2 * (lane & 3) + e);
+                c.re[h][g][e] = x.x;
+                c.im[h][g][e] = x.y;
+            }
+}
+
+// f(i, j, value) for every element of the tile at (i0, j0)
+template <class F>
+__device__ __forceinline__ void z16_store(const Z16& c, int i0, int j0, F f) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int g = 0; g < 2; ++g)
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+                f(i0 + 8 * h + (lane >> 2), j0 + 8 * g + 2 * (lane & 3) + e, c2(c.re[h][g][e], c.im[h][g][e]));
+}
+
+// c += A(i0:i0+16, k0:k1) B(k0:k1, j0:j0+16); a_at(i, k) and b_at(k, j)
+// return the operand elements (they must return 0 outside the operands;
+// k < k1 is checked here).
+template <class FA, class FB>
+__device__ __forceinline__ void z16_mma(Z16& c, int i0, int j0, int k0, int k1, FA a_at, FB b_at) {
+    const int lane = threadIdx.x & 31;
+    const int ar = i0 + (lane >> 2), bc = j0 + (lane >> 2), kq = lane & 3;
+#pragma unroll 2
+    for (int k = k0; k < k1; k += 4) {
+        const int kk = k + kq;
+        double2 a[2], b[2];
+        if (kk < k1) {
+            a[0] = a_at(ar, kk);
+            a[1] = a_at(ar + 8, kk);
+            b[0] = b_at(kk, bc);
+            b[1] = b_at(kk, bc + 8);
+        } else {
+            a[0] = a[1] = b[0] = b[1] = c2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int g = 0; g < 2; ++g) {
+                dmma(c.re[h][g], a[h].x, b[g].x);
+                dmma(c.re[h][g], -a[h].y, b[g].y);
+                dmma(c.im[h][g], a[h].x, b[g].y);
+                dmma(c.im[h][g], a[h].y, b[g].x);
+            }
+    }
+}
+
+// t -> (ti, tj) with ti >= tj, enumerating the lower triangle row by row.
+__device__ __forceinline__ void tri_tile(int t, int& ti, int& tj) {
+    int r = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+    while ((r + 1) * (r + 2) / 2 <= t) ++r;
+    while (r * (r + 1) / 2 > t) --r;
+    ti = r;
+    tj = t - r * (r + 1) / 2;
+}
+
+__global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, ld = a.ld;
+    const size_t mat = (size_t)n * ld;
+    double2* M0 = a.scratch + (size_t)blockIdx.x * tiled_slot_elems(n);
+    double2* M1 = M0 + mat;
+    double2* M2 = M1 + mat;
+    double*  Zo = reinterpret_cast<double*>(M2 + mat);
+    double2* Wsc = M2 + mat;                 // WY scratch (16 x n), shares Zo's storage
+    TVec v = tcarve(smem_raw, n);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tn = (n + 15) >> 4;
+    const size_t nn = (size_t)n * n;
+    const double2 zero = c2(0.0, 0.0);
+
+    for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) {
+        const double2* Hb = a.H + (size_t)b * nn;
+        const double2* Sb = a.S + (size_t)b * nn;
+        double*  Wb = a.W + (size_t)b * n;
+        double2* Ub = a.U + (size_t)b * nn;
+
+        __syncthreads();  // previous pencil fully consumed
+        // ---- a1: S (lower triangle and diagonal) -> M0
+        for (int idx = tid; idx < (int)nn; idx += kNT) {
+            const int j = idx / n, i = idx - j * n;
+            if (i >= j) M0[i + (size_t)j * ld] = __ldg(Sb + idx);
+        }
+        if (tid < 8) v.ctl[tid] = 0;
+        __syncthreads();
+
+        // ---- a2: blocked Cholesky (lower). The pivot test is the same as
+        // potrf's (not > 0, NaN included), taken in column order.
+        int fail = 0;
+        for (int p = 0; p < n && !fail; p += 16) {
+            const int pe = min(p + 16, n);
+            for (int c = p; c < pe; ++c) {
+                const double piv = M0[c + (size_t)c * ld].x;
+                if (!(piv > 0.0)) { fail = c + 1; break; }
+                const double lc = sqrt(piv), r = 1.0 / lc;
+                double2* lcol = M0 + (size_t)c * ld;
+                for (int i = c + 1 + tid; i < n; i += kNT) lcol[i] = cscale(lcol[i], r);
+                __syncthreads();
+                if (tid == 0) { lcol[c] = c2(lc, 0.0); v.rdg[c] = r; }
+                // rank-1 update of the panel columns right of c
+                const int wc = pe - c - 1, rows = n - c - 1;
+                for (int idx = tid; idx < rows * wc; idx += kNT) {
+                    const int cc = c + 1 + idx / rows, i = c + 1 + idx % rows;
+                    if (i >= cc) {
+                        double2* x = M0 + i + (size_t)cc * ld;
+                        *x = cfms_bc(*x, lcol[i], lcol[cc]);
+                    }
+                }
+                __syncthreads();
+            }
+            if (fail) break;
+            // trailing lower tiles: C -= L_p L_p^H over columns [p, pe)
+            const int m2 = n - pe;
+            if (m2 > 0) {
+                const int tm = (m2 + 15) >> 4, T = tm * (tm + 1) / 2;
+                for (int t = warp; t < T; t += kNW) {
+                    int ti, tj;
+                    tri_tile(t, ti, tj);
+                    const int i0 = pe + 16 * ti, j0 = pe + 16 * tj;
+                    Z16 acc;
+                    z16_load(acc, i0, j0, [&](int i, int j) { return (i < n && j < n) ? M0[i + (size_t)j * ld] : zero; });
+                    z16_mma(acc, i0, j0, p, pe,
+                            [&](int i, int k) { return i < n ? cneg(M0[i + (size_t)k * ld]) : zero; },
+                            [&](int k, int j) { return j < n ? cconj(M0[j + (size_t)k * ld]) : zero; });
+                    z16_store(acc, i0, j0, [&](int i, int j, double2 x) {
+                        if (i < n && j < n && i >= j) M0[i + (size_t)j * ld] = x;
+                    });
+                }
+            }
+            __syncthreads();
+        }
+        int code = fail ? n + fail : 0;   // zhegv: info = n + order of the failing minor
+
+        if (!code && a.stage >= 2) {
+            // ---- a3: X = L^-1 -> M1, block row r0..re at a time
+            for (int r0 = 0; r0 < n; r0 += 16) {
+                const int re = min(r0 + 16, n);
+                for (int t = warp; t < (r0 >> 4); t += kNW) {
+                    const int j0 = 16 * t;
+                    Z16 acc;
+                    z16_zero(acc);
+                    z16_mma(acc, r0, j0, j0, r0,
+                            [&](int i, int k) { return i < n ? M0[i + (size_t)k * ld] : zero; },
+                            [&](int k, int j) { return k >= j ? M1[k + (size_t)j * ld] : zero; });
+                    z16_store(acc, r0, j0, [&](int i, int j, double2 x) { if (i < n) M1[i + (size_t)j * ld] = x; });
+                }
+                __syncthreads();
+                for (int c = tid; c < re; c += kNT) {
+                    double2 x[16];
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) {
+                        const int i = r0 + r;
+                        x[r] = (i < re) ? ((c < r0) ? cneg(M1[i + (size_t)c * ld]) : c2(i == c ? 1.0 : 0.0, 0.0))
+                                        : zero;
+                    }
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) {
+                        const int i = r0 + r;
+                        if (i < re) {
+                            double2 s = x[r];
+#pragma unroll
+                            for (int q = 0; q < r; ++q) s = cfms(s, M0[i + (size_t)(r0 + q) * ld], x[q]);
+                            x[r] = cscale(s, v.rdg[i]);
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < 16; ++r)
+                        if (r0 + r < re) M1[r0 + r + (size_t)c * ld] = x[r];
+                }
+                __syncthreads();
+            }
+        }
+
+        if (!code && a.stage == 1) {
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                Ub[idx] = (i >= j) ? M0[i + (size_t)j * ld] : zero;
+            }
+            if (tid == 0) a.info[b] = 0;
+            continue;
+        }
+
+        if (!code) {
+            // ---- a4: T = H X^H -> M2, T(i, j) = sum_{k <= j} H(i, k) conj(X(j, k))
+            if (a.sigma) {
+                const int m = n >> 1;
+                for (int idx = tid; idx < (int)nn; idx += kNT) {
+                    const int j = idx / n, i = idx - j * n;
+                    const double2 x = (i <= j) ? cconj(M1[j + (size_t)i * ld]) : zero;
+                    M2[i + (size_t)j * ld] = (i < m) ? x : cneg(x);
+                }
+            } else {
+                for (int t = warp; t < tn * tn; t += kNW) {
+                    const int ti = t / tn, tj = t - ti * tn, i0 = 16 * ti, j0 = 16 * tj;
+                    Z16 acc;
+                    z16_zero(acc);
+                    z16_mma(acc, i0, j0, 0, min(n, j0 + 16),
+                            [&](int i, int k) { return i < n ? __ldg(Hb + i + (size_t)k * n) : zero; },
+                            [&](int k, int j) { return (j < n && k <= j) ? cconj(M1[j + (size_t)k * ld]) : zero; });
+                    z16_store(acc, i0, j0, [&](int i, int j, double2 x) {
+                        if (i < n && j < n) M2[i + (size_t)j * ld] = x;
+                    });
+                }
+            }
+            __syncthreads();
+            // C = X T, lower tiles; each lower element is written with its
+            // mirror so that C is exactly Hermitian. L in M0 is dead by now.
+            for (int t = warp; t < tn * (tn + 1) / 2; t += kNW) {
+                int ti, tj;
+                tri_tile(t, ti, tj);
+                const int i0 = 16 * ti, j0 = 16 * tj;
+                Z16 acc;
+                z16_zero(acc);
+                z16_mma(acc, i0, j0, 0, min(n, i0 + 16),
+                        [&](int i, int k) { return (i < n && k <= i) ? M1[i + (size_t)k * ld] : zero; },
+                        [&](int k, int j) { return j < n ? M2[k + (size_t)j * ld] : zero; });
+                z16_store(acc, i0, j0, [&](int i, int j, double2 x) {
+                    if (i < n && j < n && i >= j) {
+                        if (i == j) x.y = 0.0;
+                        M0[i + (size_t)j * ld] = x;
+                        M0[j + (size_t)i * ld] = cconj(x);
+                    }
+                });
+            }
+            __syncthreads();
+        }
+
+        if (!code && a.stage == 2) {
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                Ub[idx] = M0[i + (size_t)j * ld];
+            }
+            if (tid == 0) a.info[b] = 0;
+            continue;
+        }
+
+        if (!code) {
+            // ---- a5a: Householder tridiagonalisation of C (lower). Reflector
+            // k: I - tau_k v v^H on rows k+1.., v[k+1] = 1, v[k+2..] stored in
+            // column k of M0 below the subdiagonal (no longer part of A22).
+            for (int k = 0; k < n - 1; ++k) {
+                double2* ck = M0 + (size_t)k * ld;
+                if (warp == 0) {
+                    double ss = 0.0;
+                    for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = ck[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                    ss = warp_sum(ss);
+                    const double2 alpha = ck[k + 1];
+                    double2 taui, scal = zero;
+                    double beta;
+                    if (ss == 0.0 && alpha.y == 0.0) {
+                        taui = zero;
+                        beta = alpha.x;
+                    } else {
+                        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+                        taui = c2((beta - alpha.x) / beta, -alpha.y / beta);
+                        const double2 z = c2(alpha.x - beta, alpha.y);
+                        const double inv = 1.0 / (z.x * z.x + z.y * z.y);
+                        scal = c2(z.x * inv, -z.y * inv);
+                    }
+                    for (int i = k + 2 + lane; i < n; i += 32) {
+                        const double2 vi = cmul(ck[i], scal);
+                        v.vb[i] = vi;
+                        ck[i] = vi;
+                    }
+                    if (lane == 0) {
+                        v.vb[k + 1] = c2(1.0, 0.0);
+                        v.tau[k] = taui;
+                        v.d[k] = ck[k].x;
+                        v.e[k] = beta;
+                    }
+                }
+                __syncthreads();
+                const double2 taui = v.tau[k];
+                if (taui.x == 0.0 && taui.y == 0.0) continue;
+                // p = tau A22 v, one warp per entry: p_i = sum_j conj(A(j, i)) v_j
+                // (A22 is kept as a full Hermitian matrix, read down column i)
+                for (int i = k + 1 + warp; i < n; i += kNW) {
+                    const double2* ci = M0 + (size_t)i * ld;
+                    double2 acc = zero;
+#pragma unroll 4
+                    for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, ci[j], v.vb[j]);
+                    acc = warp_sum2(acc);
+                    if (lane == 0) v.pb[i] = cmul(taui, acc);
+                }
+                __syncthreads();
+                if (warp == 0) {
+                    double2 dot = zero;
+                    for (int i = k + 1 + lane; i < n; i += 32) dot = cfmac(dot, v.pb[i], v.vb[i]);
+                    dot = warp_sum2(dot);
+                    if (lane == 0) v.red[0] = cscale(cmul(taui, dot), -0.5);
+                }
+                __syncthreads();
+                const double2 alpha2 = v.red[0];
+                // A22 -= v w^H + w v^H, w = p + alpha2 v; a warp per column
+                for (int j = k + 1 + warp; j < n; j += kNW) {
+                    double2* cj = M0 + (size_t)j * ld;
+                    const double2 vj = v.vb[j], wj = cfma(v.pb[j], alpha2, vj);
+#pragma unroll 4
+                    for (int i = k + 1 + lane; i < n; i += 32) {
+                        const double2 vi = v.vb[i], wi = cfma(v.pb[i], alpha2, vi);
+                        double2 x = cj[i];
+                        x = cfms_bc(x, vi, wj);
+                        x = cfms_bc(x, wi, vj);
+                        cj[i] = x;
+                    }
+                }
+                __syncthreads();
+            }
+            if (tid == 0) {
+                v.d[n - 1] = M0[(n - 1) + (size_t)(n - 1) * ld].x;
+                if (n == 1) v.tau[0] = zero;
+            }
+            __syncthreads();
+
+            // ---- a5b: divide and conquer on T: Z in M2 (real), its merge
+            // workspace after it, merge products through Zo
+            DCShared dc;
+            dc.Z = reinterpret_cast<double*>(M2); dc.ldz = ld;
+            dc.U = dc.Z + mat;                    dc.ldu = ld;
+            dc.Zo = Zo;
+            dc.d = v.d; dc.e = v.e;
+            dc.w = v.dcd; dc.z = dc.w + n; dc.dl = dc.z + n; dc.zz = dc.dl + n; dc.zh = dc.zz + n;
+            dc.rt = dc.zh + n; dc.rho = dc.rt + n; dc.scal = dc.rho + n;
+            dc.org = v.dci; dc.nd = dc.org + n; dc.perm = dc.nd + n; dc.kcnt = dc.perm + n;
+            tridiag_dc<kNT, 0>(n, dc);
+            if (tid == 0) {
+                bool bad = false;
+                for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
+                v.ctl[4] = bad ? n : 0;
+            }
+            __syncthreads();
+            code = v.ctl[4];
+            if (!code) {
+                for (int j = tid; j < n; j += kNT) {
+                    const double dj = order_key(v.dcd[j]);
+                    int r = 0;
+                    for (int k2 = 0; k2 < n; ++k2) {
+                        const double dk = order_key(v.dcd[k2]);
+                        r += (dk < dj) || (dk == dj && k2 < j);
+                    }
+                    v.rank[j] = r;
+                }
+            }
+            __syncthreads();
+        }
+
+        if (code) {
+            const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+            for (int idx = tid; idx < (int)nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
+            if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
+            if (tid == 0) a.info[b] = code;
+            continue;
+        }
+
+        // ---- a5c: V = Q Z in the output, columns in ascending eigenvalue order
+        {
+            const double* Z = reinterpret_cast<const double*>(M2);
+            for (int idx = tid; idx < (int)nn; idx += kNT) {
+                const int j = idx / n, i = idx - j * n;
+                Ub[i + (size_t)v.rank[j] * n] = c2(Z[i + (size_t)j * ld], 0.0);
+            }
+            for (int j = tid; j < n; j += kNT) Wb[v.rank[j]] = v.dcd[j];
+        }
+        __syncthreads();
+        const int nref = n - 1;
+        for (int kb = nref > 0 ? ((nref - 1) / 16) * 16 : -1; kb >= 0; kb -= 16) {
+            const int w = min(16, nref - kb);
+            // Y(i, c) = v_{kb+c}(i): 0 above row kb+c+1, 1 there, stored below
+            auto Y = [&](int i, int c) -> double2 {
+                if (c >= w || i >= n) return zero;
+                const int k = kb + c;
+                return (i <= k) ? zero : (i == k + 1) ? c2(1.0, 0.0) : M0[i + (size_t)k * ld];
+            };
+            v.tb[tid] = zero;   // kNT == 256 == 16 x 16
+            // G = Y^H Y: warps 0 and 1 each sum half of the rows, and the two
+            // halves are added in a fixed order (results are bitwise
+            // reproducible from launch to launch)
+            if (warp < 2) {
+                const int r0 = kb + 1, rows = n - r0;
+                const int per = ((rows + 7) / 8) * 4;
+                const int k0 = r0 + warp * per, k1 = min(n, k0 + per);
+                Z16 acc;
+                z16_zero(acc);
+                z16_mma(acc, 0, 0, k0, k1, [&](int c, int i) { return cconj(Y(i, c)); },
+                        [&](int i, int c) { return Y(i, c); });
+                z16_store(acc, 0, 0, [&](int i, int j, double2 x) { v.gb[256 * warp + i + 16 * j] = x; });
+            }
+            __syncthreads();
+            v.gb[tid] = cadd(v.gb[tid], v.gb[256 + tid]);
+            __syncthreads();
+            // T_b (upper triangular, forward column-wise): T(j, j) = tau_j,
+            // T(0:j, j) = T(0:j, 0:j) (-tau_j G(0:j, j))
+            if (warp == 0) {
+                for (int j = 0; j < w; ++j) {
+                    const double2 tj = v.tau[kb + j];
+                    const double2 y = (lane < j) ? cneg(cmul(tj, v.gb[lane + 16 * j])) : zero;
+                    double2 s = zero;
+                    for (int l = 0; l < j; ++l) {
+                        const double2 yl = c2(__shfl_sync(0xffffffffu, y.x, l), __shfl_sync(0xffffffffu, y.y, l));
+                        if (lane <= l) s = cfma(s, v.tb[lane + 16 * l], yl);
+                    }
+                    if (lane < j) v.tb[lane + 16 * j] = s;
+                    if (lane == j) v.tb[j + 16 * j] = tj;
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            // W1 = Y^H V (16 x n) then W2 = T_b W1 in place, one column tile per warp
+            for (int t = warp; t < tn; t += kNW) {
+                const int j0 = 16 * t;
+                Z16 acc;
+                z16_zero(acc);
+                z16_mma(acc, 0, j0, kb + 1, n, [&](int c, int i) { return cconj(Y(i, c)); },
+                        [&](int i, int j) { return j < n ? Ub[i + (size_t)j * n] : zero; });
+                z16_store(acc, 0, j0, [&](int c, int j, double2 x) { if (j < n) Wsc[c + 16 * j] = x; });
+                __syncwarp();
+                Z16 acc2;
+                z16_zero(acc2);
+                z16_mma(acc2, 0, j0, 0, 16, [&](int c, int l) { return v.tb[c + 16 * l]; },
+                        [&](int l, int j) { return j < n ? Wsc[l + 16 * j] : zero; });
+                __syncwarp();
+                z16_store(acc2, 0, j0, [&](int c, int j, double2 x) { if (j < n) Wsc[c + 16 * j] = x; });
+            }
+            __syncthreads();
+            // V -= Y W2 on rows kb+1..n
+            const int rt0 = (kb + 1) >> 4, T = (tn - rt0) * tn;
+            for (int t = warp; t < T; t += kNW) {
+                const int ti = rt0 + t / tn, tj = t % tn, i0 = 16 * ti, j0 = 16 * tj;
+                Z16 acc;
+                z16_load(acc, i0, j0, [&](int i, int j) { return (i < n && j < n) ? Ub[i + (size_t)j * n] : zero; });
+                z16_mma(acc, i0, j0, 0, 16, [&](int i, int c) { return cneg(Y(i, c)); },
+                        [&](int c, int j) { return j < n ? Wsc[c + 16 * j] : zero; });
+                z16_store(acc, i0, j0, [&](int i, int j, double2 x) {
+                    if (i < n && j < n) Ub[i + (size_t)j * n] = x;
+                });
+            }
+            __syncthreads();
+        }
+
+        if (tid == 0) a.info[b] = 0;
+        if (a.stage == 3) continue;
+
+        // ---- a6: U = X^H V -> M2, U(i, j) = sum_{k >= i} conj(X(k, i)) V(k, j); then to the output
+        for (int t = warp; t < tn * tn; t += kNW) {
+            const int ti = t / tn, tj = t - ti * tn, i0 = 16 * ti, j0 = 16 * tj;
+            Z16 acc;
+            z16_zero(acc);
+            z16_mma(acc, i0, j0, i0, n,
+                    [&](int i, int k) { return (i < n && k >= i) ? cconj(M1[k + (size_t)i * ld]) : zero; },
+                    [&](int k, int j) { return j < n ? Ub[k + (size_t)j * n] : zero; });
+            z16_store(acc, i0, j0, [&](int i, int j, double2 x) { if (i < n && j < n) M2[i + (size_t)j * ld] = x; });
+        }
+        __syncthreads();
+        for (int idx = tid; idx < (int)nn; idx += kNT) {
+            const int j = idx / n, i = idx - j * n;
+            Ub[idx] = M2[i + (size_t)j * ld];
+        }
+    }
+}
+
+}  // namespace
+
+size_t tiled_vec_bytes(int n) {
+    return (size_t)n * 16 * 3 + 32 * 16 + 3 * 256 * 16 + (size_t)n * 8 * 3 + (size_t)dc_vec_doubles(n) * 8 +
+           (size_t)n * 4 + 8 * 4 + (size_t)dc_vec_ints(n) * 4;
+}
+
+cudaError_t tiled_set_attributes(size_t smem) {
+    return cudaFuncSetAttribute(geneig_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t tiled_launch(int n, int slots, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
+                         int* info, long long batch, void* scratch, cudaStream_t stream, bool sigma) {
+    if (batch <= 0) return cudaSuccess;
+    TiledArgs a;
+    a.H = static_cast<const double2*>(H);
+    a.S = static_cast<const double2*>(S);
+    a.W = W;
+    a.U = static_cast<double2*>(U);
+    a.info = info;
+    a.scratch = static_cast<double2*>(scratch);
+    a.batch = batch;
+    a.n = n;
+    a.ld = n | 1;
+    a.stage = stage;
+    a.sigma = sigma ? 1 : 0;
+    const long long grid = batch < slots ? batch : slots;
+    geneig_tiled_kernel<<<(unsigned)grid, kNT, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace sgeig

@@ -128,6 +128,16 @@ class Solver:
         if st != nat.STATUS_OK:
             raise RuntimeError(f"sunny_geneig_launch failed (status={st}): {nat.last_error()}")
 
+    def launch_sigma(self, S, W, U, info, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """Solves Sigma u = lambda S u with Sigma = diag(I_{n/2}, -I_{n/2}) (the spin-wave
+        metric); H is implied and not read. Same output layouts as `launch`."""
+        batch = self._check(S, S, W, U, info)
+        s = stream if stream is not None else torch.cuda.current_stream(S.device)
+        st = self._lib.sunny_geneig_launch_sigma(self.handle, S.data_ptr(), W.data_ptr(), U.data_ptr(),
+                                                 info.data_ptr(), int(batch), s.cuda_stream)
+        if st != nat.STATUS_OK:
+            raise RuntimeError(f"sunny_geneig_launch_sigma failed (status={st}): {nat.last_error()}")
+
     def run_kernel(self, H: torch.Tensor, S: torch.Tensor, W: Optional[torch.Tensor] = None,
                    U: Optional[torch.Tensor] = None, info: Optional[torch.Tensor] = None,
                    stream: Optional[torch.cuda.Stream] = None) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
