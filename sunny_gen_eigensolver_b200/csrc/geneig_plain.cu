@@ -26,6 +26,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 
 namespace sgeig {
@@ -399,6 +400,7 @@ __global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
 int g_smem_optin = -1;
 
 constexpr int kWideNmax = 96;
+constexpr int kCtaPreferredMaxN = 60;
 
 }  // namespace
 
@@ -425,30 +427,40 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
     if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return false; }
     g_smem_optin = optin;
 
+    // Optional override for measurements: SUNNY_GENEIG_REGIME = smem-cta |
+    // smem-wide | l2-slot picks that regime wherever it can hold n.
+    const char* force = std::getenv("SUNNY_GENEIG_REGIME");
+    const std::string want = force ? force : "";
     PlainPlan p;
     p.n = n;
     p.ld = n | 1;
     p.threads = kNT;
+    // Each kernel's dynamic shared-memory limit is set to the device maximum
+    // (not to this n's need), so that creating a handle for a smaller n never
+    // lowers the limit under a live handle for a larger one.
+    // Measured on B200 (solves/s, batch 32768): the tiled kernel overtakes the
+    // register-resident smem-cta kernel between n = 60 and n = 62 and runs
+    // about 2x the smem-wide kernel at n = 66..80, so smem-wide is only used
+    // when asked for.
     const size_t smem_wide = (size_t)2 * n * p.ld * 16 + vec_area_bytes(n);
-    if (n <= kCtaMaxN && cta_smem_bytes(n) <= (size_t)optin) {
+    const bool cta_ok = n <= kCtaMaxN && cta_smem_bytes(n) <= (size_t)optin;
+    const bool wide_ok = smem_wide <= (size_t)optin && n <= kWideNmax;
+    if (cta_ok && ((want.empty() && n <= kCtaPreferredMaxN) || want == "smem-cta")) {
         p.regime = Regime::SmemCta;
         p.smem = cta_smem_bytes(n);
         p.nmax = cta_nmax_for(n);
-        e = cta_set_attributes(p.nmax, p.smem);
+        e = cta_set_attributes(p.nmax, (size_t)optin);
+    } else if (wide_ok && want == "smem-wide") {
+        p.regime = Regime::SmemWide;
+        p.smem = smem_wide;
+        p.nmax = kWideNmax;
+        e = cudaFuncSetAttribute(geneig_plain_kernel<kWideNmax>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     } else {
-        if (smem_wide <= (size_t)optin && n <= kWideNmax) {
-            p.regime = Regime::SmemWide;
-            p.smem = smem_wide;
-            p.nmax = kWideNmax;
-            e = cudaFuncSetAttribute(geneig_plain_kernel<kWideNmax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)p.smem);
-        } else {
-            p.regime = Regime::L2Slot;
-            p.smem = tiled_vec_bytes(n);
-            p.slots = 2 * sms;
-            p.scratch_bytes = (size_t)p.slots * tiled_slot_bytes(n);
-            e = tiled_set_attributes(p.smem);
-        }
+        p.regime = Regime::L2Slot;
+        p.smem = tiled_vec_bytes(n);
+        p.slots = 2 * sms;
+        p.scratch_bytes = (size_t)p.slots * tiled_slot_bytes(n);
+        e = tiled_set_attributes((size_t)optin);
     }
     if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
     *plan = p;
@@ -515,7 +527,10 @@ cudaError_t noalloc_setup(int dev, NoAllocDevice** out, std::string* err) {
         if (e != cudaSuccess) { *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return e; }
         e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return e; }
-        e = tiled_set_attributes(tiled_vec_bytes(kMaxN));
+        int optin = 0;
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return e; }
+        e = tiled_set_attributes((size_t)optin);
         if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return e; }
         d.scratch = ptr;
         d.ready = true;

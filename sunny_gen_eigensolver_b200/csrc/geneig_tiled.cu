@@ -3,7 +3,7 @@
 // regime). One CTA solves one pencil at a time, persistent over the batch;
 // its working matrices live in a per-CTA global-memory slot
 //     M0, M1, M2: n x ld complex,  Zo: n x ld real (at least 16 n complex)
-// and every O(n^3) step except the Householder reduction is a complex GEMM
+// and every O(n^3) step except the Householder matrix-vector products is a complex GEMM
 // on the FP64 tensor cores (mma.sync.m8n8k4.f64; a complex 8x8x4 step is four
 // real MMAs), one 16 x 16 output tile per warp at a time:
 //
@@ -16,7 +16,8 @@
 //       C = L^-1 H L^-H; for the spin-wave metric H = diag(I, -I) the first
 //       product is a sign flip of X^H                              (:248)
 //   a5  C = Q T Q^H (Householder, lower; v_k kept in column k of M0 below
-//       the subdiagonal), T = Z diag(w) Z^T by divide and conquer (Z and its
+//       the subdiagonal; for n >= 96 in 16-column panels whose trailing
+//       update A -= V W^H + W V^H is a GEMM), T = Z diag(w) Z^T by divide and conquer (Z and its
 //       merge workspace in M2, merge products through Zo), V = Q Z with
 //       compact-WY blocks of 16 reflectors, Q_b = I - Y T_b Y^H:
 //       W1 = Y^H V, W2 = T_b W1, V -= Y W2 (all GEMMs), V in the output U   (:250)
@@ -36,6 +37,10 @@ namespace {
 
 constexpr int kNT = 256;          // threads per CTA
 constexpr int kNW = kNT / 32;     // warps per CTA
+// Below this n the per-column (unblocked) Householder reduction is faster on
+// B200 than the 16-column panels (fewer barriers per column); above it the
+// panels' halved trailing-matrix traffic wins (measured crossover ~90).
+constexpr int kBlockedHetrdMinN = 96;
 
 struct TiledArgs {
     const double2* __restrict__ H;
@@ -364,74 +369,209 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
         if (!code) {
             // ---- a5a: Householder tridiagonalisation of C (lower). Reflector
             // k: I - tau_k v v^H on rows k+1.., v[k+1] = 1, v[k+2..] stored in
-            // column k of M0 below the subdiagonal (no longer part of A22).
-            for (int k = 0; k < n - 1; ++k) {
-                double2* ck = M0 + (size_t)k * ld;
-                if (warp == 0) {
-                    double ss = 0.0;
-                    for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = ck[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
-                    ss = warp_sum(ss);
-                    const double2 alpha = ck[k + 1];
-                    double2 taui, scal = zero;
-                    double beta;
-                    if (ss == 0.0 && alpha.y == 0.0) {
-                        taui = zero;
-                        beta = alpha.x;
-                    } else {
-                        beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
-                        taui = c2((beta - alpha.x) / beta, -alpha.y / beta);
-                        const double2 z = c2(alpha.x - beta, alpha.y);
-                        const double inv = 1.0 / (z.x * z.x + z.y * z.y);
-                        scal = c2(z.x * inv, -z.y * inv);
+            // column k of M0 below the subdiagonal. Small n: one rank-2
+            // update of the trailing matrix per column. Larger n: blocked as
+            // LAPACK's zhetrd/zlatrd, panels of up to 16 columns reduced
+            // against the panel-start trailing matrix A with the corrections
+            // of the panel's earlier columns (V = reflectors, W = their
+            // update vectors, W kept in M2 whose product T is dead by now),
+            // then A -= V W^H + W V^H on tensor-core tiles.
+            if (n < kBlockedHetrdMinN) {
+                for (int k = 0; k < n - 1; ++k) {
+                    double2* ck = M0 + (size_t)k * ld;
+                    if (warp == 0) {
+                        double ss = 0.0;
+                        for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = ck[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                        ss = warp_sum(ss);
+                        const double2 alpha = ck[k + 1];
+                        double2 taui, scal = zero;
+                        double beta;
+                        if (ss == 0.0 && alpha.y == 0.0) {
+                            taui = zero;
+                            beta = alpha.x;
+                        } else {
+                            beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+                            taui = c2((beta - alpha.x) / beta, -alpha.y / beta);
+                            const double2 z = c2(alpha.x - beta, alpha.y);
+                            const double inv = 1.0 / (z.x * z.x + z.y * z.y);
+                            scal = c2(z.x * inv, -z.y * inv);
+                        }
+                        for (int i = k + 2 + lane; i < n; i += 32) {
+                            const double2 vi = cmul(ck[i], scal);
+                            v.vb[i] = vi;
+                            ck[i] = vi;
+                        }
+                        if (lane == 0) {
+                            v.vb[k + 1] = c2(1.0, 0.0);
+                            v.tau[k] = taui;
+                            v.d[k] = ck[k].x;
+                            v.e[k] = beta;
+                        }
                     }
-                    for (int i = k + 2 + lane; i < n; i += 32) {
-                        const double2 vi = cmul(ck[i], scal);
-                        v.vb[i] = vi;
-                        ck[i] = vi;
+                    __syncthreads();
+                    const double2 taui = v.tau[k];
+                    if (taui.x == 0.0 && taui.y == 0.0) continue;
+                    // p = tau A22 v, one warp per entry: p_i = sum_j conj(A(j, i)) v_j
+                    // (A22 is kept as a full Hermitian matrix, read down column i)
+                    for (int i = k + 1 + warp; i < n; i += kNW) {
+                        const double2* ci = M0 + (size_t)i * ld;
+                        double2 acc = zero;
+    #pragma unroll 4
+                        for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, ci[j], v.vb[j]);
+                        acc = warp_sum2(acc);
+                        if (lane == 0) v.pb[i] = cmul(taui, acc);
                     }
-                    if (lane == 0) {
-                        v.vb[k + 1] = c2(1.0, 0.0);
-                        v.tau[k] = taui;
-                        v.d[k] = ck[k].x;
-                        v.e[k] = beta;
+                    __syncthreads();
+                    if (warp == 0) {
+                        double2 dot = zero;
+                        for (int i = k + 1 + lane; i < n; i += 32) dot = cfmac(dot, v.pb[i], v.vb[i]);
+                        dot = warp_sum2(dot);
+                        if (lane == 0) v.red[0] = cscale(cmul(taui, dot), -0.5);
                     }
-                }
-                __syncthreads();
-                const double2 taui = v.tau[k];
-                if (taui.x == 0.0 && taui.y == 0.0) continue;
-                // p = tau A22 v, one warp per entry: p_i = sum_j conj(A(j, i)) v_j
-                // (A22 is kept as a full Hermitian matrix, read down column i)
-                for (int i = k + 1 + warp; i < n; i += kNW) {
-                    const double2* ci = M0 + (size_t)i * ld;
-                    double2 acc = zero;
-#pragma unroll 4
-                    for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, ci[j], v.vb[j]);
-                    acc = warp_sum2(acc);
-                    if (lane == 0) v.pb[i] = cmul(taui, acc);
-                }
-                __syncthreads();
-                if (warp == 0) {
-                    double2 dot = zero;
-                    for (int i = k + 1 + lane; i < n; i += 32) dot = cfmac(dot, v.pb[i], v.vb[i]);
-                    dot = warp_sum2(dot);
-                    if (lane == 0) v.red[0] = cscale(cmul(taui, dot), -0.5);
-                }
-                __syncthreads();
-                const double2 alpha2 = v.red[0];
-                // A22 -= v w^H + w v^H, w = p + alpha2 v; a warp per column
-                for (int j = k + 1 + warp; j < n; j += kNW) {
-                    double2* cj = M0 + (size_t)j * ld;
-                    const double2 vj = v.vb[j], wj = cfma(v.pb[j], alpha2, vj);
-#pragma unroll 4
-                    for (int i = k + 1 + lane; i < n; i += 32) {
-                        const double2 vi = v.vb[i], wi = cfma(v.pb[i], alpha2, vi);
-                        double2 x = cj[i];
-                        x = cfms_bc(x, vi, wj);
-                        x = cfms_bc(x, wi, vj);
-                        cj[i] = x;
+                    __syncthreads();
+                    const double2 alpha2 = v.red[0];
+                    // A22 -= v w^H + w v^H, w = p + alpha2 v; a warp per column
+                    for (int j = k + 1 + warp; j < n; j += kNW) {
+                        double2* cj = M0 + (size_t)j * ld;
+                        const double2 vj = v.vb[j], wj = cfma(v.pb[j], alpha2, vj);
+    #pragma unroll 4
+                        for (int i = k + 1 + lane; i < n; i += 32) {
+                            const double2 vi = v.vb[i], wi = cfma(v.pb[i], alpha2, vi);
+                            double2 x = cj[i];
+                            x = cfms_bc(x, vi, wj);
+                            x = cfms_bc(x, wi, vj);
+                            cj[i] = x;
+                        }
                     }
+                    __syncthreads();
                 }
-                __syncthreads();
+            } else {
+                double2* Wp = M2;
+                for (int p = 0; p < n - 1; p += 16) {
+                    const int w = min(16, n - 1 - p);
+                    // V(i, c) = v_{p+c}(i) for rows i > p + c
+                    auto Vp = [&](int i, int c) -> double2 {
+                        const int k = p + c;
+                        return (i <= k) ? zero : (i == k + 1) ? c2(1.0, 0.0) : M0[i + (size_t)k * ld];
+                    };
+                    for (int c = 0; c < w; ++c) {
+                        const int k = p + c;
+                        double2* ck = M0 + (size_t)k * ld;
+                        // (1) a_k(k:n) -= V(k:n, 0:c) W(k, 0:c)^H + W(k:n, 0:c) V(k, 0:c)^H
+                        if (c > 0) {
+                            for (int i = k + tid; i < n; i += kNT) {
+                                double2 x = ck[i];
+                                for (int cc = 0; cc < c; ++cc) {
+                                    x = cfms_bc(x, Vp(i, cc), Wp[k + (size_t)cc * ld]);
+                                    x = cfms_bc(x, Wp[i + (size_t)cc * ld], Vp(k, cc));
+                                }
+                                ck[i] = x;
+                            }
+                            __syncthreads();
+                        }
+                        // (2) reflector from a_k(k+1:n), warp 0
+                        if (warp == 0) {
+                            double ss = 0.0;
+                            for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = ck[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                            ss = warp_sum(ss);
+                            const double2 alpha = ck[k + 1];
+                            double2 taui, scal = zero;
+                            double beta;
+                            if (ss == 0.0 && alpha.y == 0.0) {
+                                taui = zero;
+                                beta = alpha.x;
+                            } else {
+                                beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + ss), alpha.x);
+                                taui = c2((beta - alpha.x) / beta, -alpha.y / beta);
+                                const double2 z = c2(alpha.x - beta, alpha.y);
+                                const double inv = 1.0 / (z.x * z.x + z.y * z.y);
+                                scal = c2(z.x * inv, -z.y * inv);
+                            }
+                            for (int i = k + 2 + lane; i < n; i += 32) {
+                                const double2 vi = cmul(ck[i], scal);
+                                v.vb[i] = vi;
+                                ck[i] = vi;
+                            }
+                            if (lane == 0) {
+                                v.vb[k + 1] = c2(1.0, 0.0);
+                                v.tau[k] = taui;
+                                v.d[k] = ck[k].x;
+                                v.e[k] = beta;
+                            }
+                        }
+                        __syncthreads();
+                        const double2 taui = v.tau[k];
+                        // (3) y = A v (A: panel-start trailing matrix, read down
+                        // column i: y_i = sum_j conj(A(j, i)) v_j), t1 = W^H v and
+                        // t2 = V^H v over rows k+1..n; one warp per item
+                        const int m = n - k - 1;
+                        for (int it = warp; it < m + 2 * c; it += kNW) {
+                            double2 acc = zero;
+                            if (it < m) {
+                                const int i = k + 1 + it;
+                                const double2* ci = M0 + (size_t)i * ld;
+    #pragma unroll 4
+                                for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, ci[j], v.vb[j]);
+                            } else if (it < m + c) {
+                                const double2* wc = Wp + (size_t)(it - m) * ld;
+                                for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, wc[j], v.vb[j]);
+                            } else {
+                                const int cc = it - m - c;
+                                for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, Vp(j, cc), v.vb[j]);
+                            }
+                            acc = warp_sum2(acc);
+                            if (lane == 0) {
+                                if (it < m) v.pb[k + 1 + it] = acc;
+                                else v.red[it - m] = acc;      // t1 at red[0..c), t2 at red[c..2c)
+                            }
+                        }
+                        __syncthreads();
+                        // (4) w = tau (y - V t1 - W t2) on rows k+1..n: the
+                        // current trailing matrix is A - V W^H - W V^H
+                        for (int i = k + 1 + tid; i < n; i += kNT) {
+                            double2 x = v.pb[i];
+                            for (int cc = 0; cc < c; ++cc) {
+                                x = cfms(x, Vp(i, cc), v.red[cc]);
+                                x = cfms(x, Wp[i + (size_t)cc * ld], v.red[c + cc]);
+                            }
+                            v.pb[i] = cmul(taui, x);
+                        }
+                        __syncthreads();
+                        // (5) alpha2 = -tau/2 (w^H v)
+                        if (warp == 0) {
+                            double2 dot = zero;
+                            for (int i = k + 1 + lane; i < n; i += 32) dot = cfmac(dot, v.pb[i], v.vb[i]);
+                            dot = warp_sum2(dot);
+                            if (lane == 0) v.gb[0] = cscale(cmul(taui, dot), -0.5);
+                        }
+                        __syncthreads();
+                        // (6) W(:, c) = w + alpha2 v on rows k+1..n, zero above
+                        const double2 alpha2 = v.gb[0];
+                        for (int i = tid; i < n; i += kNT)
+                            Wp[i + (size_t)c * ld] = (i > k) ? cfma(v.pb[i], alpha2, v.vb[i]) : zero;
+                        __syncthreads();
+                    }
+                    // trailing update A(q:n, q:n) -= V W^H + W V^H, q = p + w (all tiles)
+                    const int q = p + w, mq = n - q;
+                    if (mq > 0) {
+                        const int tq = (mq + 15) >> 4;
+                        for (int t = warp; t < tq * tq; t += kNW) {
+                            const int ti = t / tq, tj = t - ti * tq, i0 = q + 16 * ti, j0 = q + 16 * tj;
+                            Z16 acc;
+                            z16_load(acc, i0, j0, [&](int i, int j) { return (i < n && j < n) ? M0[i + (size_t)j * ld] : zero; });
+                            z16_mma(acc, i0, j0, 0, w,
+                                    [&](int i, int cc) { return i < n ? cneg(Vp(i, cc)) : zero; },
+                                    [&](int cc, int j) { return j < n ? cconj(Wp[j + (size_t)cc * ld]) : zero; });
+                            z16_mma(acc, i0, j0, 0, w,
+                                    [&](int i, int cc) { return i < n ? cneg(Wp[i + (size_t)cc * ld]) : zero; },
+                                    [&](int cc, int j) { return j < n ? cconj(Vp(j, cc)) : zero; });
+                            z16_store(acc, i0, j0, [&](int i, int j, double2 x) {
+                                if (i < n && j < n) M0[i + (size_t)j * ld] = x;
+                            });
+                        }
+                    }
+                    __syncthreads();
+                }
             }
             if (tid == 0) {
                 v.d[n - 1] = M0[(n - 1) + (size_t)(n - 1) * ld].x;

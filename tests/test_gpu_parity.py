@@ -78,7 +78,7 @@ def test_large_sizes_l2_slot(cuda, n):
     check_against_zhegv(H, S, W, U, info)
 
 
-@pytest.mark.parametrize("n", [1, 3, 5, 7, 33, 55])
+@pytest.mark.parametrize("n", [1, 3, 5, 7, 33, 55, 61, 97, 129])
 def test_odd_sizes(cuda, n):
     rng = np.random.default_rng(n)
     A = rng.standard_normal((5, n, n)) + 1j * rng.standard_normal((5, n, n))
@@ -145,16 +145,18 @@ def test_nan_input_reports_failure_without_hanging(cuda):
     check_against_zhegv(H[[0, 2]], S[[0, 2]], W[[0, 2]], U[[0, 2]], info[[0, 2]])
 
 
-def test_stage_cholesky(cuda):
-    H, S = generators.baseline_problems(54, 6, seed=3)
+@pytest.mark.parametrize("n", [54, 108])
+def test_stage_cholesky(cuda, n):
+    H, S = generators.baseline_problems(n, 6, seed=3)
     _, U, info = gpu_solve(H, S, stage=1)
     L, ir = zpotrf_batch(S)
     assert (info == 0).all() and (ir == 0).all()
     assert np.abs(U - L).max() <= 1e-12 * np.abs(L).max()
 
 
-def test_stage_reduce(cuda):
-    H, S = generators.baseline_problems(54, 6, seed=4)
+@pytest.mark.parametrize("n", [54, 108])
+def test_stage_reduce(cuda, n):
+    H, S = generators.baseline_problems(n, 6, seed=4)
     _, C, info = gpu_solve(H, S, stage=2)
     Cr, _, _ = reduce_batch(H, S)
     assert (info == 0).all()
@@ -162,14 +164,15 @@ def test_stage_reduce(cuda):
     assert np.array_equal(C, np.conj(np.swapaxes(C, -1, -2)))
 
 
-def test_stage_reduce_eig(cuda):
-    H, S = generators.baseline_problems(54, 6, seed=5)
+@pytest.mark.parametrize("n", [54, 108])
+def test_stage_reduce_eig(cuda, n):
+    H, S = generators.baseline_problems(n, 6, seed=5)
     W, V, info = gpu_solve(H, S, stage=3)
     Cr, _, _ = reduce_batch(H, S)
     Wr, _ = zheev_batch(Cr)
     assert (info == 0).all()
     assert accuracy.eig_err_rel(Cr, W, Wr).max() < 1e-12
-    I = np.broadcast_to(np.eye(54), Cr.shape)
+    I = np.broadcast_to(np.eye(n), Cr.shape)
     assert accuracy.residual(Cr, I, W, V).max() < 1e-12
     assert accuracy.s_orth(I, V).max() < 1e-12
 
@@ -244,3 +247,35 @@ def test_one_l2_slot_handle_on_two_streams(cuda):
         torch.cuda.synchronize()
         for sl, W, U, info in outs:
             assert torch.equal(W, Wr[sl]) and torch.equal(U, Ur[sl]) and torch.equal(info, ir[sl])
+
+
+@pytest.mark.parametrize("big,small", [(64, 50), (384, 108), (80, 66)])
+def test_smaller_handle_created_later_keeps_larger_working(cuda, big, small):
+    """Handles for a large and then a smaller N of the same kernel are both
+    usable afterwards (creating the second must not lower a launch limit the
+    first one relies on)."""
+    from sunny_gen_eigensolver_b200 import Solver
+    s_big = Solver(big)
+    s_small = Solver(small)
+    try:
+        for n, s in ((big, s_big), (small, s_small)):
+            H, S = generators.baseline_problems(n, 2, seed=n)
+            W, U, info = gpu_solve(H, S, solver=s)
+            check_against_zhegv(H, S, W, U, info)
+    finally:
+        s_small.close()
+        s_big.close()
+
+
+@pytest.mark.parametrize("n,regime", [(72, "smem-wide"), (80, "smem-wide"), (64, "smem-cta"), (54, "l2-slot"),
+                                      (18, "l2-slot"), (2, "l2-slot")])
+def test_forced_regimes_match_zhegv(cuda, monkeypatch, n, regime):
+    """Every kernel stays correct where the default choice no longer uses it
+    (SUNNY_GENEIG_REGIME forces the regime at create time)."""
+    from sunny_gen_eigensolver_b200 import Solver
+    monkeypatch.setenv("SUNNY_GENEIG_REGIME", regime)
+    with Solver(n) as s:
+        assert s.regime == regime
+        H, S = generators.baseline_problems(n, 5, seed=300 + n)
+        W, U, info = gpu_solve(H, S, solver=s)
+        check_against_zhegv(H, S, W, U, info)
