@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--e2e-chunk", type=int, default=8192)
+    p.add_argument("--kernel", choices=["unified", "mixed"], default="unified",
+                   help="mixed: FP32 Householder reduction + FP64 Ogita-Aishima refinement (kernel mode 2)")
     p.add_argument("--sigma", action="store_true",
                    help="spin-wave metric pencils: H = diag(I, -I) implied (sunny_geneig_launch_sigma), "
                         "S = the BdG matrix")
@@ -119,6 +121,7 @@ def workload_config(args, world):
                      f"{args.kappa:g}; one launch per step"),
         "n": args.n, "batch_per_gpu": args.batch, "global_batch": args.batch * world,
         "cond_S_max": args.kappa, "parallelism": f"replicas x{world}",
+        "kernel": getattr(args, "kernel", "unified"),
         "l2": "inputs 2 x batch x N^2 x 16 B >> 126 MB L2 (no flush needed)"
         if 2 * args.batch * args.n * args.n * 16 > 126e6 else "inputs fit L2: L2 flushed between steps",
     }
@@ -221,7 +224,7 @@ def run_ours(args):
     W = torch.empty((batch, n), dtype=torch.float64, device=dev)
     U = torch.empty((batch, n, n), dtype=torch.complex128, device=dev)
     info = torch.empty((batch,), dtype=torch.int32, device=dev)
-    solver = Solver(n, device_id=local)
+    solver = Solver(n, device_id=local, kernel=args.kernel)
     stream = torch.cuda.current_stream(dev)
 
     peak = measure_fp64_peak(torch, dev)
@@ -264,6 +267,21 @@ def run_ours(args):
     orth = G.abs().amax(dim=(-2, -1))
     acc = {"max_residual_upper_bound": float(res.max().item()), "max_s_orth": float(orth.max().item()),
            "failed_matrices": bad, "sorted": bool((W[:, 1:] >= W[:, :-1]).all().item())}
+    if args.kernel == "mixed":
+        # eigenvalues against the plain FP64 kernel on the same inputs (that
+        # kernel is held to LAPACK zhegv by the parity tests)
+        Wp = torch.empty_like(W)
+        Up = torch.empty_like(U)
+        ip = torch.empty_like(info)
+        with Solver(n, device_id=local) as sp:
+            if args.sigma:
+                sp.launch_sigma(S, Wp, Up, ip, stream)
+            else:
+                sp.launch(H, S, Wp, Up, ip, stream)
+            torch.cuda.synchronize(dev)
+        scale = Wp.abs().amax(dim=1).clamp_min(1e-300)
+        acc["max_eig_diff_vs_plain_rel"] = float(((W - Wp).abs().amax(dim=1) / scale).max().item())
+        del Wp, Up, ip
     del R, G, res, orth
 
     solves = batch * world * args.steps
@@ -292,7 +310,7 @@ def run_ours(args):
         out = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.kernel == "mixed" else "f64",
             "data": "synthetic (seeded BdG H / Haar-unitary S generator, generated on the device)",
             "config": workload_config(args, world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

@@ -70,7 +70,8 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
                   std::to_string(sgeig::kMaxN) + "]");
         return nullptr;
     }
-    if (mode != SUNNY_GENEIG_KERNEL_UNIFIED && mode != SUNNY_GENEIG_KERNEL_HYBRID) {
+    if (mode != SUNNY_GENEIG_KERNEL_UNIFIED && mode != SUNNY_GENEIG_KERNEL_HYBRID &&
+        mode != SUNNY_GENEIG_KERNEL_MIXED) {
         set_error(std::string(fn) + ": unsupported kernel_mode " + std::to_string((int)mode));
         return nullptr;
     }
@@ -101,7 +102,8 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
     (void)bpb_request;
     std::string err;
     e = with_device(device_id, [&]() -> cudaError_t {
-        if (!sgeig::plain_plan(n, device_id, &s->plan, &err)) return cudaErrorInvalidValue;
+        if (!sgeig::plain_plan(n, device_id, &s->plan, &err, mode == SUNNY_GENEIG_KERNEL_MIXED))
+            return cudaErrorInvalidValue;
         if (s->plan.scratch_bytes) {
             cudaError_t ea = cudaMalloc(&s->scratch, s->plan.scratch_bytes);
             if (ea != cudaSuccess) { err = std::string("cudaMalloc scratch: ") + cudaGetErrorString(ea); return ea; }

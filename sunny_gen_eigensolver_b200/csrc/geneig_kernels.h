@@ -29,19 +29,29 @@ cudaError_t cta_set_attributes(int nmax, size_t smem);
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
                        int* info, long long batch, cudaStream_t stream, bool sigma = false);
 
-// Tiled kernel for the L2Slot regime (geneig_tiled.cu). A CTA's slot holds
-// three n x ld complex matrices and one real one (at least 16 n complex), in
-// double2 units:
-__host__ __device__ inline size_t tiled_slot_elems(int n) {
+// Tiled kernel for the L2Slot regime (geneig_tiled.cu). A CTA's slot holds,
+// in double2 units, three n x ld complex matrices (four in the mixed form)
+// and an n x ld real one (at least 16 n complex); the mixed form adds an
+// n x ld single-precision complex copy of C.
+__host__ __device__ inline size_t tiled_zo_elems(int n) {
     const size_t mat = (size_t)n * (size_t)(n | 1);
-    const size_t zo = (mat + 1) / 2 > (size_t)16 * n ? (mat + 1) / 2 : (size_t)16 * n;
-    return 3 * mat + zo;
+    return (mat + 1) / 2 > (size_t)16 * n ? (mat + 1) / 2 : (size_t)16 * n;
 }
-__host__ __device__ inline size_t tiled_slot_bytes(int n) { return tiled_slot_elems(n) * 16; }
+__host__ __device__ inline size_t tiled_slot_elems(int n, bool mixed = false) {
+    const size_t mat = (size_t)n * (size_t)(n | 1);
+    return (mixed ? 4 : 3) * mat + tiled_zo_elems(n) + (mixed ? (mat + 1) / 2 : 0);
+}
+__host__ __device__ inline size_t tiled_slot_bytes(int n, bool mixed = false) {
+    return tiled_slot_elems(n, mixed) * 16;
+}
 size_t tiled_vec_bytes(int n);
 cudaError_t tiled_set_attributes(size_t smem);
+// `mixed`: FP32 Householder reduction, FP64 refinement (see geneig_tiled.cu).
+// `refine_max`: mixed form's refinement steps before it falls back to FP64.
+constexpr int kRefineMaxIters = 8;
 cudaError_t tiled_launch(int n, int slots, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
-                         int* info, long long batch, void* scratch, cudaStream_t stream, bool sigma);
+                         int* info, long long batch, void* scratch, cudaStream_t stream, bool sigma,
+                         bool mixed = false, int refine_max = kRefineMaxIters);
 
 struct PlainPlan {
     int    n        = 0;
@@ -52,11 +62,15 @@ struct PlainPlan {
     int    nmax     = 0;      // SmemCta: compile-time row bound of the register arrays
     int    slots    = 0;      // L2Slot: number of resident CTAs (= scratch slots)
     size_t scratch_bytes = 0; // L2Slot: bytes of device scratch needed
+    bool   mixed    = false;  // mixed-precision form (always the L2Slot regime)
+    int    refine_max = kRefineMaxIters;  // mixed: refinement steps before the FP64 fallback
 };
 
 // Picks the regime and launch shape for size n on `device` and sets the
 // kernel attributes it needs. Returns false with a message on failure.
-bool plain_plan(int n, int device, PlainPlan* plan, std::string* err);
+// `mixed` selects the mixed-precision form (FP32 Householder reduction plus
+// FP64 eigenpair refinement), which runs in the L2Slot regime for every n.
+bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed = false);
 
 // Enqueues one launch of `stage` (1..4) over `batch` matrices on `stream`.
 // `scratch` must hold plan.scratch_bytes when plan.regime == L2Slot.

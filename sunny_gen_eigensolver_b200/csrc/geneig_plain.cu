@@ -415,7 +415,7 @@ int smem_cta_max_n() {
     return best;
 }
 
-bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
+bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed) {
     if (n < 1 || n > kMaxN) {
         *err = "matrix size out of range [1, " + std::to_string(kMaxN) + "]";
         return false;
@@ -445,12 +445,19 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
     const size_t smem_wide = (size_t)2 * n * p.ld * 16 + vec_area_bytes(n);
     const bool cta_ok = n <= kCtaMaxN && cta_smem_bytes(n) <= (size_t)optin;
     const bool wide_ok = smem_wide <= (size_t)optin && n <= kWideNmax;
-    if (cta_ok && ((want.empty() && n <= kCtaPreferredMaxN) || want == "smem-cta")) {
+    p.mixed = mixed;
+    // SUNNY_GENEIG_MIXED_REFINE_MAX caps the mixed form's refinement steps
+    // (0..32); pencils that have not converged by then are solved in FP64.
+    if (const char* rm = std::getenv("SUNNY_GENEIG_MIXED_REFINE_MAX")) {
+        const int v = std::atoi(rm);
+        p.refine_max = v < 0 ? 0 : v > 32 ? 32 : v;
+    }
+    if (!mixed && cta_ok && ((want.empty() && n <= kCtaPreferredMaxN) || want == "smem-cta")) {
         p.regime = Regime::SmemCta;
         p.smem = cta_smem_bytes(n);
         p.nmax = cta_nmax_for(n);
         e = cta_set_attributes(p.nmax, (size_t)optin);
-    } else if (wide_ok && want == "smem-wide") {
+    } else if (!mixed && wide_ok && want == "smem-wide") {
         p.regime = Regime::SmemWide;
         p.smem = smem_wide;
         p.nmax = kWideNmax;
@@ -459,7 +466,7 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err) {
         p.regime = Regime::L2Slot;
         p.smem = tiled_vec_bytes(n);
         p.slots = 2 * sms;
-        p.scratch_bytes = (size_t)p.slots * tiled_slot_bytes(n);
+        p.scratch_bytes = (size_t)p.slots * tiled_slot_bytes(n, mixed);
         e = tiled_set_attributes((size_t)optin);
     }
     if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return false; }
@@ -485,7 +492,8 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const 
     if (plan.regime == Regime::SmemCta)
         return cta_launch(plan.n, plan.nmax, plan.smem, stage, H, S, W, U, info, batch, stream, sigma);
     if (plan.regime == Regime::L2Slot)
-        return tiled_launch(plan.n, plan.slots, plan.smem, stage, H, S, W, U, info, batch, scratch, stream, sigma);
+        return tiled_launch(plan.n, plan.slots, plan.smem, stage, H, S, W, U, info, batch, scratch, stream, sigma,
+                            plan.mixed, plan.refine_max);
     const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
     geneig_plain_kernel<kWideNmax><<<(unsigned)grid, kNT, plan.smem, stream>>>(a);
     return cudaGetLastError();

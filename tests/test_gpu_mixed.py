@@ -1,0 +1,121 @@
+"""Mixed-precision form (kernel mode MIXED): FP32 Householder reduction of
+C = L^-1 H L^-H, FP64 divide and conquer and back-transform, then FP64
+Ogita-Aishima refinement steps of the eigenpairs of C (until the correction
+is below 1e-10), then U = L^-H V.
+
+Held to the same bars as the plain FP64 kernel, against LAPACK zhegv on the
+same inputs: eigenvalues within 1e-12 ||H||_2, identical info codes, and
+residual / ||U^H S U - I|| within max(1e-12, 4x zhegv's own value on the same
+problem). The relative floor matters at cond(S) = 1e5, where FP64 zhegv
+itself reaches residuals of ~5e-12 (the error of any FP64 solve grows with
+cond(S)). Swept over S condition numbers 1e1, 1e3, 1e5 (the mixed-vs-plain
+workload's sweep) and several sizes, for both kernels.
+"""
+import numpy as np
+import pytest
+
+from oracle import zhegv_batch
+from sunny_gen_eigensolver_b200 import accuracy, generators
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_solve(H, S, stage=4, kernel="mixed"):
+    import torch
+    from sunny_gen_eigensolver_b200 import Solver, solve
+    with Solver(H.shape[-1], kernel=kernel) as s:
+        if kernel == "mixed":
+            assert s.kernel_mode == "mixed" and s.path_name == "mixed" and s.regime == "l2-slot"
+        W, U, info = solve(torch.from_numpy(np.ascontiguousarray(H)).cuda(),
+                           torch.from_numpy(np.ascontiguousarray(S)).cuda(), solver=s, stage=stage)
+    return W.cpu().numpy(), U.cpu().numpy(), info.cpu().numpy()
+
+
+@pytest.mark.parametrize("kernel", ["mixed", "unified"])
+@pytest.mark.parametrize("n", [2, 12, 54, 128])
+@pytest.mark.parametrize("kappa", [1e1, 1e3, 1e5])
+def test_matches_zhegv_over_cond_S(cuda, n, kappa, kernel):
+    H, S = generators.baseline_problems(n, 6, seed=500 + n, kappa=kappa)
+    W, U, info = mixed_solve(H, S, kernel=kernel)
+    Wr, Ur, ir = zhegv_batch(H, S)
+    assert np.array_equal(info, ir) and (ir == 0).all()
+    assert accuracy.eig_err_rel(H, W, Wr).max() <= 1e-12
+    r, rr = accuracy.residual(H, S, W, U), accuracy.residual(H, S, Wr, Ur)
+    o, orr = accuracy.s_orth(S, U), accuracy.s_orth(S, Ur)
+    assert (r <= np.maximum(1e-12, 4 * rr)).all(), (r.max(), rr.max())
+    assert (o <= np.maximum(1e-12, 4 * orr)).all(), (o.max(), orr.max())
+    assert (np.diff(W, axis=-1) >= 0).all()
+
+
+def test_mixed_odd_size_and_degenerate_spectrum(cuda):
+    n = 33
+    rng = np.random.default_rng(7)
+    X = rng.standard_normal((3, n, n)) + 1j * rng.standard_normal((3, n, n))
+    Q, _ = np.linalg.qr(X)
+    lam = np.repeat(np.arange(11, dtype=float), 3)          # 3-fold clusters
+    H = (Q * lam[None, None, :]) @ np.conj(np.swapaxes(Q, -1, -2))
+    H = 0.5 * (H + np.conj(np.swapaxes(H, -1, -2)))
+    S = np.broadcast_to(np.eye(n, dtype=np.complex128), H.shape).copy()
+    W, U, info = mixed_solve(H, S)
+    Wr, _, _ = zhegv_batch(H, S)
+    assert (info == 0).all()
+    assert accuracy.eig_err_rel(H, W, Wr).max() <= 1e-12
+    assert accuracy.residual(H, S, W, U).max() <= 1e-12
+    assert accuracy.s_orth(S, U).max() <= 1e-12
+
+
+def test_mixed_stage3_vectors_of_C(cuda):
+    from oracle import reduce_batch, zheev_batch
+    n = 64
+    H, S = generators.baseline_problems(n, 4, seed=31)
+    W, V, info = mixed_solve(H, S, stage=3)
+    Cr, _, _ = reduce_batch(H, S)
+    Wr, _ = zheev_batch(Cr)
+    I = np.broadcast_to(np.eye(n), Cr.shape)
+    assert (info == 0).all()
+    assert accuracy.eig_err_rel(Cr, W, Wr).max() < 1e-12
+    assert accuracy.residual(Cr, I, W, V).max() < 1e-12
+    assert accuracy.s_orth(I, V).max() < 1e-12
+
+
+def test_mixed_non_pd_info_and_determinism(cuda):
+    import torch
+    from sunny_gen_eigensolver_b200 import Solver, to_colmajor
+    n = 54
+    H, S = generators.baseline_problems(n, 7, seed=2)
+    S[3] = np.eye(n)
+    S[3, 20, 20] = 0.0                       # leading minor 21 singular: info = n + 21
+    _, _, ir = zhegv_batch(H, S)
+    with Solver(n, kernel="mixed") as s:
+        Ht = to_colmajor(torch.from_numpy(H).cuda())
+        St = to_colmajor(torch.from_numpy(S).cuda())
+        W1, U1, i1 = s.run_kernel(Ht, St)
+        W2, U2, i2 = s.run_kernel(Ht, St)
+        torch.cuda.synchronize()
+        # bit for bit, NaN fills of the failed matrix included
+        bits = lambda t: torch.view_as_real(t).view(torch.int64) if t.is_complex() else t.view(torch.int64)
+        assert torch.equal(bits(W1), bits(W2)) and torch.equal(bits(U1), bits(U2)) and torch.equal(i1, i2)
+    info = i1.cpu().numpy()
+    assert np.array_equal(info, ir) and info[3] == n + 21
+    assert np.isnan(W1[3].cpu().numpy()).all()
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_mixed_fallback_equals_plain_fp64_kernel(cuda, monkeypatch, n):
+    """A pencil whose refinement does not converge is solved again in FP64
+    from C. With the refinement cap at 0 every pencil takes that path, which
+    must then give the plain kernel's results bit for bit (same tiled kernel,
+    same inputs, n >= 61)."""
+    import torch
+    from sunny_gen_eigensolver_b200 import Solver, to_colmajor
+    H, S = generators.baseline_problems(n, 5, seed=41 + n, kappa=1e5)
+    Ht = to_colmajor(torch.from_numpy(H).cuda())
+    St = to_colmajor(torch.from_numpy(S).cuda())
+    with Solver(n) as sp:
+        assert sp.regime == "l2-slot"
+        Wp, Up, ip = sp.run_kernel(Ht, St)
+    monkeypatch.setenv("SUNNY_GENEIG_MIXED_REFINE_MAX", "0")
+    with Solver(n, kernel="mixed") as sm:
+        Wm, Um, im = sm.run_kernel(Ht, St)
+    torch.cuda.synchronize()
+    assert torch.equal(Wp, Wm) and torch.equal(Up, Um) and torch.equal(ip, im)
