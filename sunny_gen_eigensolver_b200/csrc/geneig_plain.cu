@@ -465,7 +465,11 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed
     } else {
         p.regime = Regime::L2Slot;
         p.smem = tiled_vec_bytes(n);
-        p.slots = 2 * sms;
+        // resident CTAs (and scratch slots) per SM: SUNNY_GENEIG_SLOTS_PER_SM
+        // = 1 or 2 (default 2, the kernel's occupancy limit)
+        int per_sm = 2;
+        if (const char* ps = std::getenv("SUNNY_GENEIG_SLOTS_PER_SM")) per_sm = std::atoi(ps) == 1 ? 1 : 2;
+        p.slots = per_sm * sms;
         p.scratch_bytes = (size_t)p.slots * tiled_slot_bytes(n, mixed);
         e = tiled_set_attributes((size_t)optin);
     }

@@ -100,10 +100,16 @@ def poisson_requests(rate_hz: float, duration_s: float, sizes, q_range=(64, 4096
 class ServingEngine:
     """FIFO admission by slot and device-memory budget; see module docstring."""
 
-    def __init__(self, executor, budget_bytes: int = 150 * 10 ** 9, max_in_flight: Optional[int] = None):
+    def __init__(self, executor, budget_bytes: int = 150 * 10 ** 9, max_in_flight: Optional[int] = None,
+                 consume=None):
+        """`consume(request, result)`, when given, receives each finished
+        request's result (W, U, info on the device) at completion, like a
+        client reading its answer, and the engine keeps nothing of it;
+        otherwise the result stays on the request (`Request.result`)."""
         self.ex = executor
         self.budget = int(budget_bytes)
         self.slots = max_in_flight or executor.slots
+        self.consume = consume
 
     def run(self, requests: List[Request], realtime: bool = True) -> ServeStats:
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
@@ -128,7 +134,11 @@ class ServingEngine:
             for r, h in in_flight:
                 if self.ex.finished(h):
                     r.done = clock() - t0
-                    r.result = self.ex.result(h)
+                    res = self.ex.result(h)
+                    if self.consume is not None:
+                        self.consume(r, res)
+                    else:
+                        r.result = res
                     used -= request_bytes(r.n, r.q)
                     st.completed += 1
                     st.solves += r.q

@@ -71,3 +71,14 @@ def test_results_identical_alone_and_in_the_mix(cuda):
         W1, U1, i1 = alone.result
         assert torch.equal(info, i1) and bool((info == 0).all())
         assert torch.equal(W, W1) and torch.equal(U, U1)
+
+
+def test_consumer_receives_every_result_once_and_nothing_is_kept():
+    reqs = poisson_requests(200.0, 0.5, [18, 54], q_range=(64, 256), seed=3)
+    got = []
+    eng = ServingEngine(SimExecutor({18: 1e6, 54: 2e5}, slots=4), budget_bytes=10 ** 9,
+                        consume=lambda r, res: got.append((r.rid, res)))
+    st = eng.run(reqs)
+    assert st.completed == len(reqs) and sorted(rid for rid, _ in got) == sorted(r.rid for r in reqs)
+    assert all(res == rid for rid, res in got)          # SimExecutor's result is the request id
+    assert all(r.result is None for r in reqs)
