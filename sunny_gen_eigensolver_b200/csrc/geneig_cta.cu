@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             __syncthreads();   // B is free from here on
             if (j < n) {
 #pragma unroll
-                for (int c = NMAX / 16 - 1; c >= 0; --c) {
+                for (int c = (NMAX + 15) / 16 - 1; c >= 0; --c) {
                     const int khi = min(16 * c + 15, n - 2);
                     for (int k = khi; k >= 16 * c; --k) {
                         const double2 tk = v.tau[k];
@@ -553,7 +553,9 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
 
 size_t cta_smem_bytes(int n) { return (size_t)2 * n * (n | 1) * 16 + cta_vec_bytes(n); }
 
-int cta_nmax_for(int n) { return n <= 16 ? 16 : n <= 32 ? 32 : n <= 48 ? 48 : 64; }
+// Compile-time row bounds: the register arrays and unrolled loops are sized by
+// NMAX, so a bound close above n wastes less (56 covers the N=54 workload).
+int cta_nmax_for(int n) { return n <= 16 ? 16 : n <= 32 ? 32 : n <= 48 ? 48 : n <= 56 ? 56 : 64; }
 
 using CtaKernelFn = void (*)(CtaArgs);
 static CtaKernelFn cta_kernel_for(int nmax) {
@@ -561,6 +563,7 @@ static CtaKernelFn cta_kernel_for(int nmax) {
         case 16: return geneig_cta_kernel<16>;
         case 32: return geneig_cta_kernel<32>;
         case 48: return geneig_cta_kernel<48>;
+        case 56: return geneig_cta_kernel<56>;
         default: return geneig_cta_kernel<64>;
     }
 }

@@ -64,7 +64,7 @@ def test_reference_fixtures(cuda, golden, name):
         assert accuracy.phase_err(S[:2], U[:2], rec["U2"], rec["W"][:2]).max() < 1e-10
 
 
-@pytest.mark.parametrize("n", [2, 4, 12, 18, 24, 54, 72, 80, 108, 128])
+@pytest.mark.parametrize("n", [2, 4, 12, 18, 24, 50, 54, 56, 72, 80, 108, 128])
 def test_baseline_generator_sizes(cuda, n):
     H, S = generators.baseline_problems(n, 16, seed=20261203 + n)
     W, U, info = gpu_solve(H, S)
