@@ -463,6 +463,20 @@ def run_uneven(args):
     steps = max(1, args.steps // 4)
     t_graph = timed(ub.replay, steps)
     t_seq = timed(ub.run_sequential, steps)
+    # one plain launch per size with the library's default configuration per N
+    from sunny_gen_eigensolver_b200 import Solver
+    defaults = {n: Solver(n) for n in ub.counts}
+    cur = torch.cuda.current_stream()
+
+    def run_default():
+        for n, s in defaults.items():
+            s.launch(ub.H[n], ub.S[n], ub.W[n], ub.U[n], ub.info[n], cur)
+
+    t_def = timed(run_default, steps)
+    for s in defaults.values():
+        s.close()
+    ub.replay()                        # leave the tuned results in the buffers for the checks
+    torch.cuda.synchronize()
     bad = sum(int((ub.info[n] != 0).sum().item()) for n in ub.counts)
     flops = sum(flops_per_solve(n) * c for n, c in ub.counts.items())
     out = {"metric": METRIC, "mode": "uneven", "value": ub.total / t_graph, "unit": "solves/s",
@@ -472,6 +486,8 @@ def run_uneven(args):
                       "counts": {str(n): c for n, c in ub.counts.items()}},
            "graph_solves_per_s": ub.total / t_graph, "sequential_solves_per_s": ub.total / t_seq,
            "graph_speedup": t_seq / t_graph, "plan_streams": plan.streams,
+           "sequential_default_config_solves_per_s": ub.total / t_def,
+           "size_configs": {str(n): c for n, c in (plan.configs or {}).items()},
            "achieved_fp64_tflops": flops / t_graph / 1e12, "failed_matrices": bad,
            "regimes": {str(n): ub.solvers[n].regime for n in ub.counts}}
     print(json.dumps(out), flush=True)

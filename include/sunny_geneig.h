@@ -162,6 +162,16 @@ sunny_geneig_status_t sunny_geneig_launch_sigma(
     int                   batch_size,
     uintptr_t             stream);
 
+/* Create with an explicit execution configuration (no counterpart in the
+ * reference; its NVRTC autotuner picked launch shapes inside create).
+ * `regime` is "smem-cta", "smem-wide" or "l2-slot" (NULL or "" = the default
+ * choice by N); `slots_per_sm` is 1 or 2 resident CTAs per SM for the
+ * l2-slot regime (0 = default). A configuration that cannot hold n returns
+ * NULL with the reason in sunny_geneig_last_error(). The uneven-batch
+ * autotuner times the candidates per N through this call. */
+sunny_geneig_solver_t sunny_geneig_create_config(int n, int device_id, sunny_geneig_kernel_mode_t kernel_mode,
+                                                 const char* regime, int slots_per_sm);
+
 /* Largest N this build accepts in sunny_geneig_create. */
 int sunny_geneig_max_matrix_size(void);
 

@@ -29,7 +29,7 @@ EXPORTS = (
     "sunny_geneig_shared_mem_bytes", "sunny_geneig_last_error", "sunny_geneig_path_name",
     "sunny_geneig_kernel_mode", "sunny_geneig_launch_stage", "sunny_geneig_max_matrix_size",
     "sunny_geneig_regime_name", "sunny_geneig_selftest_reciprocal", "sunny_geneig_launch_noalloc",
-    "sunny_geneig_launch_sigma",
+    "sunny_geneig_launch_sigma", "sunny_geneig_create_config",
 )
 
 _lib = None
@@ -56,6 +56,8 @@ def load() -> ctypes.CDLL:
     L.sunny_geneig_create.restype = c_void_p
     L.sunny_geneig_create_ex.argtypes = [c_int] * 6
     L.sunny_geneig_create_ex.restype = c_void_p
+    L.sunny_geneig_create_config.argtypes = [c_int, c_int, c_int, ctypes.c_char_p, c_int]
+    L.sunny_geneig_create_config.restype = c_void_p
     L.sunny_geneig_destroy.argtypes = [c_void_p]
     L.sunny_geneig_destroy.restype = None
     L.sunny_geneig_launch.argtypes = [c_void_p, c_size, c_size, c_size, c_size, c_size, c_int, c_size]

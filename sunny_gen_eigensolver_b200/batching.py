@@ -7,13 +7,15 @@ of launches is captured once into a CUDA graph, so that a batch of the same
 shape is re-run by a single graph launch (`UnevenBatch.replay`). The plain
 alternative (`run_sequential`) is one launch per size on one stream.
 
-The launch plan (how many streams, which sizes share a stream, in which
-order) is picked by `autotune`: it times every size class alone, spreads the
-classes over k streams by longest-processing-time-first for each candidate
-k, captures and times each candidate graph, and keeps the fastest. Choices
-are remembered per size mix in an on-disk table (`TuneTable`), written
-atomically (temporary file + rename) and validated when read; a corrupt or
-foreign file is ignored and rewritten.
+`autotune` picks, per size class, the execution configuration (which kernel
+regime and, for the l2-slot kernel, how many CTAs per SM: `size_configs`)
+by timing every candidate that can hold that N on the class's own data, and
+then the launch plan (how many streams, which sizes share a stream, in which
+order): it spreads the classes over k streams by longest-processing-time-
+first for each candidate k, captures and times each candidate graph, and
+keeps the fastest. Choices are remembered per size mix in an on-disk table
+(`TuneTable`), written atomically (temporary file + rename) and validated
+when read; a corrupt or foreign file is ignored and rewritten.
 """
 from __future__ import annotations
 
@@ -24,7 +26,18 @@ from dataclasses import dataclass
 from pathlib import Path
 from typing import Dict, List, Optional, Sequence
 
-TABLE_VERSION = 1
+TABLE_VERSION = 2
+
+
+def size_configs(n: int) -> List[dict]:
+    """Execution configurations tried for size n (those that cannot hold n
+    are rejected by the library at create time and skipped)."""
+    cands = [{"regime": "l2-slot", "slots_per_sm": 2}, {"regime": "l2-slot", "slots_per_sm": 1}]
+    if n <= 64:
+        cands.insert(0, {"regime": "smem-cta", "slots_per_sm": 0})
+    elif n <= 96:
+        cands.append({"regime": "smem-wide", "slots_per_sm": 0})
+    return cands
 
 
 def default_table_path() -> Path:
@@ -46,9 +59,10 @@ def mix_key(counts: Dict[int, int], device_name: str = "") -> str:
 @dataclass
 class Plan:
     streams: List[List[int]]      # sizes launched on each stream, in order
+    configs: Dict[int, dict] = None   # size -> {"regime": str, "slots_per_sm": int}
 
     def to_json(self):
-        return {"streams": self.streams}
+        return {"streams": self.streams, "configs": {str(n): c for n, c in (self.configs or {}).items()}}
 
     @staticmethod
     def from_json(d) -> "Plan":
@@ -61,7 +75,13 @@ class Plan:
             st.append(list(lane))
         if not st:
             raise ValueError("empty plan")
-        return Plan(st)
+        cfg = {}
+        for k, c in (d.get("configs") or {}).items():
+            if (not isinstance(c, dict) or c.get("regime") not in ("smem-cta", "smem-wide", "l2-slot")
+                    or c.get("slots_per_sm") not in (0, 1, 2)):
+                raise ValueError("bad size config")
+            cfg[int(k)] = {"regime": c["regime"], "slots_per_sm": c["slots_per_sm"]}
+        return Plan(st, cfg)
 
 
 class TuneTable:
@@ -151,6 +171,7 @@ class UnevenBatch:
             self.solvers[n] = Solver(n, device_id=self.dev.index or 0)
         self.graph = None
         self.plan: Optional[Plan] = None
+        self.configs: Dict[int, dict] = {}
 
     @property
     def total(self) -> int:
@@ -159,6 +180,15 @@ class UnevenBatch:
     def set_inputs(self, n: int, H, S) -> None:
         self.H[n].copy_(H)
         self.S[n].copy_(S)
+
+    def use_config(self, n: int, cfg: dict) -> None:
+        """Replace size n's solver by one created with execution config `cfg`."""
+        from .solver import Solver
+        s = Solver(n, device_id=self.dev.index or 0, regime=cfg["regime"], slots_per_sm=cfg["slots_per_sm"])
+        self.solvers[n].close()
+        self.solvers[n] = s
+        self.configs[n] = dict(cfg)
+        self.graph = None
 
     def _launch(self, n, stream):
         self.solvers[n].launch(self.H[n], self.S[n], self.W[n], self.U[n], self.info[n], stream)
@@ -226,11 +256,32 @@ class UnevenBatch:
         key = mix_key(self.counts, name)
         if table is not None:
             known = table.get(key)
-            if known is not None and sorted(x for l in known.streams for x in l) == sorted(self.counts):
+            if (known is not None and sorted(x for l in known.streams for x in l) == sorted(self.counts)
+                    and sorted(known.configs or {}) == sorted(self.counts)):
+                for n, cfg in known.configs.items():
+                    self.use_config(n, cfg)
                 self.capture(known)
                 return known
+        from .solver import Solver
         cur = torch.cuda.current_stream(self.dev)
-        cost = {n: self._time(lambda n=n: self._launch(n, cur), reps=1) for n in self.counts}
+        cost = {}
+        for n in self.counts:                      # per size: fastest execution config on its own data
+            best_cfg, best_t = None, float("inf")
+            for cfg in size_configs(n):
+                try:
+                    cand = Solver(n, device_id=self.dev.index or 0, regime=cfg["regime"],
+                                  slots_per_sm=cfg["slots_per_sm"])
+                except RuntimeError:               # this config cannot hold n
+                    continue
+                try:
+                    t = self._time(lambda: cand.launch(self.H[n], self.S[n], self.W[n], self.U[n],
+                                                       self.info[n], cur), reps=2)
+                finally:
+                    cand.close()
+                if t < best_t:
+                    best_cfg, best_t = cfg, t
+            self.use_config(n, best_cfg)
+            cost[n] = best_t
         best, best_t = None, float("inf")
         seen = set()
         for k in candidates:
@@ -243,6 +294,7 @@ class UnevenBatch:
             t = self._time(self.replay, reps=3)
             if t < best_t:
                 best, best_t = plan, t
+        best.configs = dict(self.configs)
         self.capture(best)
         if table is not None:
             table.put(key, best)

@@ -63,7 +63,8 @@ bool aligned(uintptr_t p, uintptr_t a) { return (p % a) == 0; }
 sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
                                   sunny_geneig_tuning_mode_t tuning,
                                   sunny_geneig_cache_mode_t cache,
-                                  sunny_geneig_kernel_mode_t mode, const char* fn) {
+                                  sunny_geneig_kernel_mode_t mode, const char* fn,
+                                  const char* regime = nullptr, int slots_per_sm = 0) {
     clear_error();
     if (n < 1 || n > sgeig::kMaxN) {
         set_error(std::string(fn) + ": n=" + std::to_string(n) + " outside [1, " +
@@ -102,7 +103,8 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
     (void)bpb_request;
     std::string err;
     e = with_device(device_id, [&]() -> cudaError_t {
-        if (!sgeig::plain_plan(n, device_id, &s->plan, &err, mode == SUNNY_GENEIG_KERNEL_MIXED))
+        if (!sgeig::plain_plan(n, device_id, &s->plan, &err, mode == SUNNY_GENEIG_KERNEL_MIXED, regime,
+                               slots_per_sm))
             return cudaErrorInvalidValue;
         if (s->plan.scratch_bytes) {
             cudaError_t ea = cudaMalloc(&s->scratch, s->plan.scratch_bytes);
@@ -235,6 +237,17 @@ void sunny_geneig_destroy(sunny_geneig_solver_t solver) {
         }
         delete solver;
     } catch (...) {
+    }
+}
+
+sunny_geneig_solver_t sunny_geneig_create_config(int n, int device_id, sunny_geneig_kernel_mode_t kernel_mode,
+                                                 const char* regime, int slots_per_sm) {
+    try {
+        return create_impl(n, device_id, 0, SUNNY_GENEIG_TUNING_SUGGESTED, SUNNY_GENEIG_CACHE_AUTO, kernel_mode,
+                           "sunny_geneig_create_config", regime, slots_per_sm);
+    } catch (...) {
+        set_error("unknown C++ exception in sunny_geneig_create_config");
+        return nullptr;
     }
 }
 

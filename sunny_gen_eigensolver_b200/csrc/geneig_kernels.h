@@ -70,7 +70,12 @@ struct PlainPlan {
 // kernel attributes it needs. Returns false with a message on failure.
 // `mixed` selects the mixed-precision form (FP32 Householder reduction plus
 // FP64 eigenpair refinement), which runs in the L2Slot regime for every n.
-bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed = false);
+// `regime` (smem-cta | smem-wide | l2-slot) and `slots_per_sm` (1 or 2, the
+// l2-slot CTAs per SM) request a configuration explicitly; a request that
+// cannot hold n fails with a message. NULL / "" and 0 keep the default
+// choice (or the SUNNY_GENEIG_REGIME / SUNNY_GENEIG_SLOTS_PER_SM overrides).
+bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed = false,
+                const char* regime = nullptr, int slots_per_sm = 0);
 
 // Enqueues one launch of `stage` (1..4) over `batch` matrices on `stream`.
 // `scratch` must hold plan.scratch_bytes when plan.regime == L2Slot.

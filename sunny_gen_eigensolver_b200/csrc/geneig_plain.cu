@@ -415,7 +415,8 @@ int smem_cta_max_n() {
     return best;
 }
 
-bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed) {
+bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed, const char* regime,
+                int slots_per_sm) {
     if (n < 1 || n > kMaxN) {
         *err = "matrix size out of range [1, " + std::to_string(kMaxN) + "]";
         return false;
@@ -429,8 +430,17 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed
 
     // Optional override for measurements: SUNNY_GENEIG_REGIME = smem-cta |
     // smem-wide | l2-slot picks that regime wherever it can hold n.
-    const char* force = std::getenv("SUNNY_GENEIG_REGIME");
+    const bool asked = regime != nullptr && regime[0] != '\0';
+    const char* force = asked ? regime : std::getenv("SUNNY_GENEIG_REGIME");
     const std::string want = force ? force : "";
+    if (asked && want != "smem-cta" && want != "smem-wide" && want != "l2-slot") {
+        *err = "unknown regime '" + want + "' (smem-cta, smem-wide or l2-slot)";
+        return false;
+    }
+    if (slots_per_sm != 0 && slots_per_sm != 1 && slots_per_sm != 2) {
+        *err = "slots_per_sm must be 0 (default), 1 or 2";
+        return false;
+    }
     PlainPlan p;
     p.n = n;
     p.ld = n | 1;
@@ -446,6 +456,10 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed
     const bool cta_ok = n <= kCtaMaxN && cta_smem_bytes(n) <= (size_t)optin;
     const bool wide_ok = smem_wide <= (size_t)optin && n <= kWideNmax;
     p.mixed = mixed;
+    if (asked && ((want == "smem-cta" && (mixed || !cta_ok)) || (want == "smem-wide" && (mixed || !wide_ok)))) {
+        *err = "regime " + want + " cannot hold n=" + std::to_string(n) + (mixed ? " in the mixed form" : "");
+        return false;
+    }
     // SUNNY_GENEIG_MIXED_REFINE_MAX caps the mixed form's refinement steps
     // (0..32); pencils that have not converged by then are solved in FP64.
     if (const char* rm = std::getenv("SUNNY_GENEIG_MIXED_REFINE_MAX")) {
@@ -468,7 +482,8 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed
         // resident CTAs (and scratch slots) per SM: SUNNY_GENEIG_SLOTS_PER_SM
         // = 1 or 2 (default 2, the kernel's occupancy limit)
         int per_sm = 2;
-        if (const char* ps = std::getenv("SUNNY_GENEIG_SLOTS_PER_SM")) per_sm = std::atoi(ps) == 1 ? 1 : 2;
+        if (slots_per_sm != 0) per_sm = slots_per_sm;
+        else if (const char* ps = std::getenv("SUNNY_GENEIG_SLOTS_PER_SM")) per_sm = std::atoi(ps) == 1 ? 1 : 2;
         p.slots = per_sm * sms;
         p.scratch_bytes = (size_t)p.slots * tiled_slot_bytes(n, mixed);
         e = tiled_set_attributes((size_t)optin);

@@ -37,14 +37,25 @@ class Solver:
     """Owns one libsunny_geneig handle (SunnyGeneigBench.jl:37-57)."""
 
     def __init__(self, n: int, *, device_id: int = 0, bpb_request: int = 0, tuning: str = "suggested",
-                 cache: str = "auto", kernel: str = "unified"):
+                 cache: str = "auto", kernel: str = "unified", regime: Optional[str] = None,
+                 slots_per_sm: int = 0):
+        """`regime` ("smem-cta", "smem-wide", "l2-slot") and `slots_per_sm` (1, 2)
+        request an execution configuration through sunny_geneig_create_config;
+        by default the library chooses by n."""
         L = nat.load()
         tuning_int = nat.TUNING_AUTOTUNE if tuning == "autotune" else nat.TUNING_SUGGESTED
         cache_int = {"nodisk": nat.CACHE_NODISK, "nocache": nat.CACHE_NOCACHE}.get(cache, nat.CACHE_AUTO)
         kernel_int = {"hybrid": nat.KERNEL_HYBRID, "mixed": nat.KERNEL_MIXED}.get(kernel, nat.KERNEL_UNIFIED)
-        h = L.sunny_geneig_create_ex(int(n), int(device_id), int(bpb_request), tuning_int, cache_int, kernel_int)
+        if regime or slots_per_sm:
+            h = L.sunny_geneig_create_config(int(n), int(device_id), kernel_int,
+                                             (regime or "").encode(), int(slots_per_sm))
+            fn = "sunny_geneig_create_config"
+        else:
+            h = L.sunny_geneig_create_ex(int(n), int(device_id), int(bpb_request), tuning_int, cache_int,
+                                         kernel_int)
+            fn = "sunny_geneig_create_ex"
         if not h:
-            raise RuntimeError(f"sunny_geneig_create_ex failed: {nat.last_error()}")
+            raise RuntimeError(f"{fn} failed: {nat.last_error()}")
         self._lib = L
         self.handle = h
         self.n = int(n)

@@ -40,25 +40,53 @@ def test_mix_key_rounds_counts():
     assert mix_key({54: 16384, 12: 60000}) == mix_key({12: 60400, 54: 16300})
 
 
+def test_plan_size_configs_roundtrip_and_validation(tmp_path):
+    from sunny_gen_eigensolver_b200.batching import size_configs
+    path = tmp_path / "plans.json"
+    key = mix_key({54: 100, 216: 10}, "dev")
+    cfg = {54: {"regime": "smem-cta", "slots_per_sm": 0}, 216: {"regime": "l2-slot", "slots_per_sm": 2}}
+    TuneTable(path).put(key, Plan([[216], [54]], cfg))
+    got = TuneTable(path).get(key)
+    assert got.configs == cfg and got.streams == [[216], [54]]
+    raw = json.loads(path.read_text())
+    raw["plans"][key]["configs"]["54"]["regime"] = "warp-magic"
+    path.write_text(json.dumps(raw))
+    assert TuneTable(path).rejected
+    raw["version"] = 1                                      # tables from the previous format are ignored
+    path.write_text(json.dumps(raw))
+    assert TuneTable(path).rejected
+    assert size_configs(54)[0]["regime"] == "smem-cta" and len(size_configs(54)) == 3
+    assert all(c["regime"] == "l2-slot" for c in size_configs(216))
+    assert {"regime": "smem-wide", "slots_per_sm": 0} in size_configs(72)
+
+
 @pytest.mark.gpu
 def test_graph_replay_matches_per_size_launches(cuda, tmp_path):
+    """autotune picks a configuration per size and a stream plan; one graph
+    replay then gives exactly what one launch per size with the same
+    configurations gives, twice in a row, and the results meet the zhegv
+    bars."""
     import torch
-    from sunny_gen_eigensolver_b200 import generators
+    from oracle import zhegv_batch
+    from sunny_gen_eigensolver_b200 import accuracy, generators
     from sunny_gen_eigensolver_b200.batching import UnevenBatch
     rng = np.random.default_rng(3)
     sizes = rng.choice([12, 24, 54, 72, 108], size=300, p=[0.3, 0.2, 0.25, 0.15, 0.1])
     ub = UnevenBatch(sizes)
+    inputs = {}
     for n, c in ub.counts.items():
         H, S = generators.baseline_problems(n, c, seed=n)
+        inputs[n] = (H, S)
         ub.set_inputs(n, torch.from_numpy(H).cuda().transpose(-1, -2), torch.from_numpy(S).cuda().transpose(-1, -2))
-    ub.run_sequential()
-    torch.cuda.synchronize()
-    ref = {n: (ub.W[n].clone(), ub.U[n].clone(), ub.info[n].clone()) for n in ub.counts}
-    for n in ub.counts:
-        ub.W[n].zero_(); ub.U[n].zero_(); ub.info[n].fill_(-1)
     table = TuneTable(tmp_path / "plans.json")
     plan = ub.autotune(table)
     assert sorted(x for lane in plan.streams for x in lane) == sorted(ub.counts)
+    assert sorted(plan.configs) == sorted(ub.counts)
+    for n, cfg in plan.configs.items():
+        assert ub.solvers[n].regime == cfg["regime"]
+    ub.run_sequential()
+    torch.cuda.synchronize()
+    ref = {n: (ub.W[n].clone(), ub.U[n].clone(), ub.info[n].clone()) for n in ub.counts}
     for n in ub.counts:
         ub.W[n].zero_(); ub.U[n].zero_(); ub.info[n].fill_(-1)
     ub.replay()
@@ -67,5 +95,12 @@ def test_graph_replay_matches_per_size_launches(cuda, tmp_path):
     for n in ub.counts:
         assert torch.equal(ub.W[n], ref[n][0]) and torch.equal(ub.U[n], ref[n][1]) and torch.equal(ub.info[n], ref[n][2])
         assert bool((ub.info[n] == 0).all())
-    # the chosen plan was persisted and is reused
-    assert TuneTable(tmp_path / "plans.json").get(mix_key(ub.counts, torch.cuda.get_device_name())) is not None
+        H, S = inputs[n]
+        W = ub.W[n].cpu().numpy()
+        U = ub.U[n].transpose(-1, -2).cpu().numpy()
+        Wr, _, _ = zhegv_batch(H, S)
+        assert accuracy.eig_err_rel(H, W, Wr).max() <= 1e-12
+        assert accuracy.residual(H, S, W, U).max() <= 1e-12
+    # the chosen plan and configurations were persisted and are reused
+    known = TuneTable(tmp_path / "plans.json").get(mix_key(ub.counts, torch.cuda.get_device_name()))
+    assert known is not None and known.configs == plan.configs

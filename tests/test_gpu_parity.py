@@ -279,3 +279,16 @@ def test_forced_regimes_match_zhegv(cuda, monkeypatch, n, regime):
         H, S = generators.baseline_problems(n, 5, seed=300 + n)
         W, U, info = gpu_solve(H, S, solver=s)
         check_against_zhegv(H, S, W, U, info)
+
+
+def test_create_config_explicit_and_rejected(cuda):
+    from sunny_gen_eigensolver_b200 import Solver
+    with Solver(54, regime="l2-slot", slots_per_sm=1) as s:
+        assert s.regime == "l2-slot"
+        H, S = generators.baseline_problems(54, 3, seed=12)
+        W, U, info = gpu_solve(H, S, solver=s)
+        check_against_zhegv(H, S, W, U, info)
+    for kw, msg in (({"regime": "smem-cta"}, "cannot hold"), ({"regime": "bogus"}, "unknown regime"),
+                    ({"slots_per_sm": 3}, "slots_per_sm")):
+        with pytest.raises(RuntimeError, match=msg):
+            Solver(100, **kw)
