@@ -14,10 +14,12 @@ constexpr int kMaxN = 512;
 int smem_cta_max_n();
 
 // How one solve is laid out on the device.
+// Default choice by N: SmemCta up to 60, L2Slot above (measured crossovers);
+// SmemWide only when asked for.
 enum class Regime : int {
-    SmemCta  = 0,  // N <= 64: both matrices in one CTA's shared memory, GEMM-tiled kernel
-    SmemWide = 1,  // N <= 83: both matrices in shared memory, column-group kernel
-    L2Slot   = 2,  // both matrices in a per-CTA global-memory slot (L2 resident)
+    SmemCta  = 0,  // N <= 64: both matrices in one CTA's shared memory, register/MMA kernel
+    SmemWide = 1,  // N <= ~80: both matrices in shared memory, column-group kernel
+    L2Slot   = 2,  // any N: working matrices in a per-CTA global-memory slot, tiled MMA kernel
 };
 
 // Shared-memory kernel for N <= 64 (geneig_cta.cu).
