@@ -35,9 +35,33 @@ def flops_per_solve(n: int) -> float:
     return 68.0 / 3.0 * n ** 3
 
 
-def hbm_bytes_per_solve(n: int) -> int:
-    # read H, S; write U (16 B each), W (8 B), info (4 B)
-    return 48 * n * n + 8 * n + 4
+def hbm_bytes_per_solve(n: int, sigma: bool = False) -> int:
+    # read H, S; write U (16 B each), W (8 B), info (4 B); the metric solve
+    # never reads H
+    return (32 if sigma else 48) * n * n + 8 * n + 4
+
+
+def eig_err_vs_zhegv(H, S, W, n_sample: int = 512, seed: int = 20261206) -> dict:
+    """Eigenvalues of a fixed random sample of the bench's matrices against
+    LAPACK zhegv (scipy's OpenBLAS, itype=1, jobz='N', uplo='L') on the host:
+    max |W - W_zhegv| / ||H||_2 over the sample. H, S, W are the device
+    buffers in column-major layout (H[b] holds matrix b transposed)."""
+    import numpy as np
+    from scipy.linalg import lapack
+    batch = W.shape[0]
+    idx = np.sort(np.random.default_rng(seed).choice(batch, size=min(n_sample, batch), replace=False))
+    import torch
+    it = torch.from_numpy(idx).to(W.device)
+    Hs = H.index_select(0, it).transpose(-1, -2).cpu().numpy()
+    Ss = S.index_select(0, it).transpose(-1, -2).cpu().numpy()
+    Ws = W.index_select(0, it).cpu().numpy()
+    worst = 0.0
+    for b in range(len(idx)):
+        w, _, inf = lapack.zhegv(Hs[b], Ss[b], itype=1, jobz="N", uplo="L")
+        if inf != 0:
+            return {"max_eig_err_vs_zhegv": None, "zhegv_info_nonzero": int(inf)}
+        worst = max(worst, float(np.abs(Ws[b] - w).max() / np.linalg.norm(Hs[b], 2)))
+    return {"max_eig_err_vs_zhegv": worst, "eig_check_sample": len(idx)}
 
 
 def parse():
@@ -84,6 +108,7 @@ def run_reference(args):
     from oracle.cpu_baseline import ZhegvPool
     per_worker = 16
     pool = ZhegvPool(args.n, per_worker=per_worker, kappa=args.kappa)
+    solved_per_step = per_worker * pool.workers
     try:
         for _ in range(max(args.warmup, 1)):
             pool.step()
@@ -102,7 +127,10 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args, world),
+        "config": dict(workload_config(args, world), reference_solves_per_step=solved_per_step,
+                       reference_sample=(f"each step solves {solved_per_step} problems of this workload's "
+                                         f"distribution ({pool.workers} workers x {per_worker}), not the "
+                                         f"whole batch")),
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": ("the reference's GPU paths need NVIDIA MathDx/cuSolverDx, absent offline; its own CPU "
@@ -277,6 +305,8 @@ def run_ours(args):
         del G
     acc = {"max_residual_upper_bound": res_max, "max_s_orth": orth_max,
            "failed_matrices": bad, "sorted": bool((W[:, 1:] >= W[:, :-1]).all().item())}
+    if rank == 0:
+        acc.update(eig_err_vs_zhegv(H, S, W))
     if args.kernel == "mixed":
         # eigenvalues against the plain FP64 kernel on the same inputs (that
         # kernel is held to LAPACK zhegv by the parity tests)
@@ -300,8 +330,8 @@ def run_ours(args):
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 via torch.matmul (best of 4)",
                 "traffic": None,
-                "algorithmic_bytes_per_launch": hbm_bytes_per_solve(n) * batch,
-                "achieved_hbm_gbs": hbm_bytes_per_solve(n) * batch / per_launch / 1e9}
+                "algorithmic_bytes_per_launch": hbm_bytes_per_solve(n, args.sigma) * batch,
+                "achieved_hbm_gbs": hbm_bytes_per_solve(n, args.sigma) * batch / per_launch / 1e9}
     tfile = REPO / "profiles" / f"dram_traffic_n{n}.json"
     if tfile.exists() and not args.sigma:
         try:

@@ -94,9 +94,11 @@ void sunny_geneig_destroy(sunny_geneig_solver_t solver);
  * LAUNCH_ERROR when the CUDA launch itself fails. One handle may be used
  * from several streams: for sizes whose solver keeps scratch slots (the
  * "l2-slot" regime) a launch on a different stream than the previous one
- * waits for it on the device, so launches of one such handle never overlap
- * (while a stream is being captured into a CUDA graph this ordering is left
- * to the graph: capture each such handle's launches on one stream). */
+ * waits for it on the device, so launches of one such handle never overlap.
+ * A launch captured into a CUDA graph takes part in the same ordering when
+ * the graph is replayed (it waits for the handle's latest use enqueued
+ * before the replay and marks its own end for later launches); inside one
+ * graph, capture each such handle's launches on one stream. */
 sunny_geneig_status_t sunny_geneig_launch(
     sunny_geneig_solver_t solver,
     uintptr_t             d_H,
@@ -192,12 +194,16 @@ sunny_geneig_status_t sunny_geneig_selftest_reciprocal(uintptr_t d_x, uintptr_t 
  * that forbid cudaMalloc from plugins, graph-replay setups that must not
  * touch the allocator. Same buffers, layouts, info codes and error
  * behaviour as sunny_geneig_launch, on the calling thread's current device,
- * with no handle: it runs the L2-slot kernel with its per-CTA scratch taken
- * from a fixed 32 MiB device array built into the library (held by every
- * GPU that loads the library until the process exits), so it allocates
- * nothing. n outside [1, 512] is rejected with INVALID_ARG. The first call
- * on a device resolves the array's address and sets the kernel's
- * shared-memory limit; make that first call before any stream capture.
+ * with no handle. For n <= 60 it runs the shared-memory kernel, which needs
+ * no scratch at all; above that, the L2-slot kernel with its per-CTA scratch
+ * taken from a fixed 32 MiB device array built into the library (held by
+ * every GPU that loads the library until the process exits), so it
+ * allocates nothing. The array holds floor(32 MiB / slot) slots, so the
+ * number of CTAs in flight, and with it the throughput, falls as n grows:
+ * 161 at n = 61, 12 at n = 216, 2 at n = 512 (a regular handle keeps two
+ * per SM). n outside [1, 512] is rejected with INVALID_ARG. The first call
+ * on a device resolves the array's address and sets the kernels'
+ * shared-memory limits; make that first call before any stream capture.
  * All calls share the one array: calls whose kernels overlap on the GPU
  * (other streams, other host threads) race on it and must be serialised by
  * the caller. */

@@ -21,8 +21,8 @@
 // Output layout: column-major N x N per matrix, batch-contiguous
 // (element (i, j) of matrix b at b*N*N + j*N + i), interleaved re/im doubles.
 //
-// Built by oracle/build_oracle.sh into oracle/_build/libgeig_fixture.so and
-// loaded with ctypes from tests/ only.
+// Built by build() in oracle/fixtures.py into oracle/_build/libgeig_fixture.so
+// and loaded with ctypes by the tests only.
 
 #include <complex>
 #include <cstdint>

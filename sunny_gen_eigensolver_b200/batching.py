@@ -258,10 +258,16 @@ class UnevenBatch:
             known = table.get(key)
             if (known is not None and sorted(x for l in known.streams for x in l) == sorted(self.counts)
                     and sorted(known.configs or {}) == sorted(self.counts)):
-                for n, cfg in known.configs.items():
-                    self.use_config(n, cfg)
-                self.capture(known)
-                return known
+                try:
+                    for n, cfg in known.configs.items():
+                        self.use_config(n, cfg)
+                except RuntimeError:
+                    # a stored configuration this build cannot create (an older
+                    # table, another regime limit): tune again and overwrite it
+                    known = None
+                if known is not None:
+                    self.capture(known)
+                    return known
         from .solver import Solver
         cur = torch.cuda.current_stream(self.dev)
         cost = {}

@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG_DIR = Path(__file__).resolve().parent
@@ -16,6 +17,8 @@ REPO_DIR = PKG_DIR.parent
 CSRC = PKG_DIR / "csrc"
 LIB_DIR = PKG_DIR / "lib"
 LIB_PATH = LIB_DIR / "libsunny_geneig.so"
+# profiling variant: same kernels with the clock64 phase timers compiled in
+TIMERS_LIB_PATH = LIB_DIR / "libsunny_geneig_timers.so"
 INCLUDE = REPO_DIR / "include"
 
 SOURCES = ["geneig_cta.cu", "geneig_plain.cu", "geneig_tiled.cu", "selftest.cu", "c_api.cpp"]
@@ -34,41 +37,54 @@ def _nvcc() -> str:
     return cand if Path(cand).exists() else "nvcc"
 
 
-def _stale() -> bool:
-    if not LIB_PATH.exists():
+def _stale(lib: Path = LIB_PATH) -> bool:
+    if not lib.exists():
         return True
-    t = LIB_PATH.stat().st_mtime
+    t = lib.stat().st_mtime
     deps = [CSRC / s for s in SOURCES + HEADERS] + [INCLUDE / "sunny_geneig.h", Path(__file__)]
     return any(p.stat().st_mtime > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> Path:
-    """Compile the sources into lib/libsunny_geneig.so (skipped when up to date)."""
-    if not force and not _stale():
-        return LIB_PATH
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False,
+          phase_timers: bool = False) -> Path:
+    """Compile the sources into lib/libsunny_geneig.so (skipped when up to date).
+
+    `phase_timers` builds the profiling variant lib/libsunny_geneig_timers.so
+    instead (-DSGEIG_PHASE_TIMERS: per-phase clock64 counters, read with
+    sunny_geneig_phase_cycles; see phase_timers.py)."""
+    lib = TIMERS_LIB_PATH if phase_timers else LIB_PATH
+    if not force and not _stale(lib):
+        return lib
     LIB_DIR.mkdir(parents=True, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
+    extra = ["-DSGEIG_PHASE_TIMERS"] if phase_timers else []
     for src in SOURCES:
-        obj = LIB_DIR / (Path(src).stem + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / src), "-o", str(obj)]
+        obj = LIB_DIR / (Path(src).stem + (".timers.o" if phase_timers else ".o"))
+        cmd = [_nvcc(), *NVCC_FLAGS, *extra, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / src), "-o", str(obj)]
         if ptxas_verbose and src.endswith(".cu"):
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
-    tmp = LIB_PATH.with_suffix(".so.tmp")
+    # the translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            sys.stderr.write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args, r.stdout, r.stderr)
+    tmp = lib.with_suffix(".so.tmp")
     cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(tmp), *objs,
            "-Xcompiler", "-fvisibility=hidden"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
-    os.replace(tmp, LIB_PATH)
+    os.replace(tmp, lib)
     for o in objs:
         Path(o).unlink(missing_ok=True)
-    return LIB_PATH
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True, ptxas_verbose="--ptxas" in sys.argv)
-    print(LIB_PATH)
+    print(build(force="--force" in sys.argv, verbose=True, ptxas_verbose="--ptxas" in sys.argv,
+                phase_timers="--phase-timers" in sys.argv))

@@ -117,4 +117,34 @@ __host__ __device__ __forceinline__ double fast_rcp(double x) {
 // LAPACK dlamch convention: eps = 2^-53 (relative machine precision).
 constexpr double kEps    = 1.1102230246251565e-16;
 
+// ---------------------------------------------------------------- phase timers
+// Profiling builds only (-DSGEIG_PHASE_TIMERS, built as a separate library by
+// build.py --phase-timers): thread 0 of every CTA adds the clock64 cycles
+// since its previous mark to the counter of the phase that just ended. Marks
+// sit right after CTA barriers, so a counter divided by the number of solves
+// is the CTA time per solve spent in that phase (with the SM shared by the
+// other resident CTAs, as in a normal run). The product library compiles
+// every mark to nothing.
+constexpr int kPhaseSlots = 32;
+#ifdef SGEIG_PHASE_TIMERS
+static __device__ unsigned long long g_phase_cycles[kPhaseSlots];
+__device__ __forceinline__ long long& phase_prev() {
+    __shared__ long long t;
+    return t;
+}
+__device__ __forceinline__ void phase_start() {
+    if (threadIdx.x == 0) phase_prev() = clock64();
+}
+__device__ __forceinline__ void phase_mark(int slot) {
+    if (threadIdx.x == 0) {
+        const long long t = clock64();
+        atomicAdd(&g_phase_cycles[slot], (unsigned long long)(t - phase_prev()));
+        phase_prev() = t;
+    }
+}
+#else
+__device__ __forceinline__ void phase_start() {}
+__device__ __forceinline__ void phase_mark(int) {}
+#endif
+
 }  // namespace sgeig

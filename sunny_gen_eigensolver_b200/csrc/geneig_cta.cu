@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
     const unsigned gmask = 0xFu << (lane & ~3);
     const size_t nn = (size_t)n * n;
 
+    phase_start();
     for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) {
         const double2* Hb = a.H + (size_t)b * nn;
         const double2* Sb = a.S + (size_t)b * nn;
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         double2* Ub = a.U + (size_t)b * nn;
 
         __syncthreads();
+        phase_mark(8);
         // ---- a1: load (rows by tc so that global reads are contiguous)
         for (int j = tr; j < n; j += 16)
             for (int i = tc; i < n; i += 16) {
@@ -191,6 +193,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         // register known at compile time.
         int fail = 0;
         __syncthreads();   // the loads above are complete
+        phase_mark(0);
         {
             const int i = g;
             double2 x[R];
@@ -253,6 +256,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             }
         }
         __syncthreads();
+        phase_mark(1);
         int code = fail ? n + fail : 0;   // zhegv: info = n + order of the failing minor
 
         if (!code && a.stage == 1) {
@@ -290,6 +294,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                     [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
                 __syncthreads();
             }
+            phase_mark(2);
             // ---- a4: C = X T, C(i, j) = sum_{k <= i} X(i, k) T(k, j); lower
             // tiles only, each lower element written with its mirror, so that
             // C is exactly Hermitian.
@@ -310,6 +315,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                         }
                     });
                 __syncthreads();
+                phase_mark(3);
             }
         }
 
@@ -427,6 +433,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             }
             if (tid == 0) v.d[n - 1] = B[(n - 1) + (size_t)(n - 1) * ld].x;
             __syncthreads();
+            phase_mark(4);
             // ---- a5b: divide and conquer; Z (real) and its workspace in B
             DCShared dc;
             dc.Z = reinterpret_cast<double*>(B); dc.ldz = ld;
@@ -442,6 +449,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                 v.ctl[4] = bad ? n : 0;
             }
             __syncthreads();
+            phase_mark(5);
             if (v.ctl[4]) code = v.ctl[4];
         }
 
@@ -516,6 +524,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             }
         }
         __syncthreads();
+        phase_mark(6);
         if (a.stage == 3) {
             for (int jj = tr; jj < n; jj += 16) {
                 double2* uo = Ub + (size_t)v.rank[jj] * n;
@@ -539,6 +548,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             ztiles_store<MAXT>(acc, tn8, tn8, [](int, int) { return true; },
                 [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
             __syncthreads();
+            phase_mark(7);
         }
         // ---- a7: store U, column j to position rank[j]
         for (int jj = tr; jj < n; jj += 16) {
@@ -591,3 +601,22 @@ cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, c
 }
 
 }  // namespace sgeig
+
+#ifdef SGEIG_PHASE_TIMERS
+// Profiling builds only: copies the per-phase cycle counters of the
+// smem-cta kernel (see phase_mark in geneig_common.cuh) to `out` and, when
+// `reset` is nonzero, clears them. Not part of the product library's ABI.
+#pragma GCC visibility push(default)
+extern "C" int sunny_geneig_phase_cycles(unsigned long long* out, int count, int reset) {
+    if (count > sgeig::kPhaseSlots) count = sgeig::kPhaseSlots;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && out && count > 0)
+        e = cudaMemcpyFromSymbol(out, sgeig::g_phase_cycles, sizeof(unsigned long long) * count);
+    if (e == cudaSuccess && reset) {
+        static const unsigned long long zeros[sgeig::kPhaseSlots] = {};
+        e = cudaMemcpyToSymbol(sgeig::g_phase_cycles, zeros, sizeof(zeros));
+    }
+    return e == cudaSuccess ? 0 : -1;
+}
+#pragma GCC visibility pop
+#endif

@@ -366,6 +366,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
         s.Z[i + j * s.ldz] = (i == j) ? 1.0 : 0.0;
     }
     __syncthreads();
+    phase_mark(10);
 
     for (int half = 1; half < n; half <<= 1) {
         const int span = half << 1;
@@ -460,6 +461,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
             }
         }
         __syncthreads();
+        phase_mark(11);
         // ---- phase B: secular roots, four lanes per root (root slot = tid / 4)
         for (int p0 = 0; p0 < 4 * n; p0 += NT) {
             const int pidx = (p0 + tid) >> 2, qq = tid & 3;
@@ -474,6 +476,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
             if (qq == 0) { s.rt[pidx] = t; s.org[pidx] = o; }
         }
         __syncthreads();
+        phase_mark(12);
         // ---- phase C: Loewner z-hat, four lanes per root
         for (int p0 = 0; p0 < 4 * n; p0 += NT) {
             const int pidx = (p0 + tid) >> 2, qq = tid & 3;
@@ -495,6 +498,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
             if (qq == 0) s.zh[pidx] = copysign(sqrt(fmax(-W, 0.0)), s.zz[pidx]);
         }
         __syncthreads();
+        phase_mark(13);
         // ---- phase D: eigenvector columns of the rank-one problem (four lanes
         // per column), new eigenvalues
         for (int p0 = 0; p0 < 4 * n; p0 += NT) {
@@ -519,6 +523,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
             if (qq == 0) s.w[s.nd[a + j]] = base + tj;
         }
         __syncthreads();
+        phase_mark(14);
         // ---- phase E: Z(:, nd) <- Z(:, nd) * U.
         if constexpr (NMAX > 0) {
             if (span >= n) dc_merge_top_regs<NT, NMAX>(n, s);
@@ -528,6 +533,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
             else dc_merge_tiled<NT>(n, half, span, s);
         }
         __syncthreads();
+        phase_mark(15);
     }
     // ---- back to the caller's units
     const double inv = 1.0 / sc;

@@ -524,10 +524,15 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const 
 // Callers that cannot allocate device memory -- code running inside another
 // framework's memory pool or under a strict no-allocation policy, plugins
 // whose host forbids cudaMalloc on its streams, and graph-replay setups that
-// must not touch the allocator -- get the L2-slot kernel with its per-CTA
-// scratch slots taken from the fixed array below instead of a cudaMalloc'd
-// buffer. The array is sized once (kNoAllocScratchBytes) and every GPU that
-// loads the library keeps it for the life of the process.
+// must not touch the allocator -- get, for n up to the smem-cta limit, the
+// shared-memory kernel, which needs no scratch at all, and above it the
+// L2-slot kernel with its per-CTA scratch slots taken from the fixed array
+// below instead of a cudaMalloc'd buffer. The array is sized once
+// (kNoAllocScratchBytes) and every GPU that loads the library keeps it for
+// the life of the process. It holds floor(32 MiB / slot) slots, so the
+// number of resident CTAs, and with it the throughput, falls with n: 161
+// CTAs at n = 61, 12 at n = 216, 2 at n = 512 (the regular launch keeps
+// 2 per SM, 296 on B200).
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;   // 32 MiB per device
@@ -537,6 +542,7 @@ struct NoAllocDevice {
     bool ready = false;
     void* scratch = nullptr;   // device address of g_noalloc_scratch on this device
     int sms = 0;
+    int optin = 0;             // largest dynamic shared memory per CTA
 };
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
@@ -544,7 +550,7 @@ NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
 
 // Once per device, with that device current: resolve the array's device
 // address (the host-side symbol is only a stand-in and must never be handed
-// to a kernel) and set the kernel's shared-memory limit.
+// to a kernel) and set the kernels' shared-memory limits.
 cudaError_t noalloc_setup(int dev, NoAllocDevice** out, std::string* err) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     NoAllocDevice& d = g_noalloc_dev[dev];
@@ -558,7 +564,10 @@ cudaError_t noalloc_setup(int dev, NoAllocDevice** out, std::string* err) {
         e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return e; }
         e = tiled_set_attributes((size_t)optin);
+        for (int nmax : {16, 32, 48, 56, 64})
+            if (e == cudaSuccess) e = cta_set_attributes(nmax, (size_t)optin);
         if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return e; }
+        d.optin = optin;
         d.scratch = ptr;
         d.ready = true;
     }
@@ -594,8 +603,13 @@ extern "C" sunny_geneig_status_t sunny_geneig_launch_noalloc(int n, uintptr_t d_
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    if (e != cudaSuccess) {
         api_set_error(std::string("sunny_geneig_launch_noalloc: no usable current device: ") + cudaGetErrorString(e));
+        return SUNNY_GENEIG_DEVICE_ERROR;
+    }
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        api_set_error("sunny_geneig_launch_noalloc: current device index " + std::to_string(dev) +
+                      " is beyond this entry point's limit of " + std::to_string(kNoAllocMaxDevices) + " devices");
         return SUNNY_GENEIG_DEVICE_ERROR;
     }
     NoAllocDevice* d = nullptr;
@@ -603,6 +617,18 @@ extern "C" sunny_geneig_status_t sunny_geneig_launch_noalloc(int n, uintptr_t d_
     if (noalloc_setup(dev, &d, &err) != cudaSuccess) {
         api_set_error("sunny_geneig_launch_noalloc: " + err);
         return SUNNY_GENEIG_DEVICE_ERROR;
+    }
+    if (n <= kCtaPreferredMaxN && cta_smem_bytes(n) <= (size_t)d->optin) {
+        // the shared-memory kernel keeps everything on chip: no scratch at all
+        e = cta_launch(n, cta_nmax_for(n), cta_smem_bytes(n), 4, reinterpret_cast<const void*>(d_H),
+                       reinterpret_cast<const void*>(d_S), reinterpret_cast<double*>(d_W),
+                       reinterpret_cast<void*>(d_U), reinterpret_cast<int*>(d_info), batch_size,
+                       reinterpret_cast<cudaStream_t>(stream), false);
+        if (e != cudaSuccess) {
+            api_set_error(std::string("sunny_geneig_launch_noalloc: kernel launch failed: ") + cudaGetErrorString(e));
+            return SUNNY_GENEIG_LAUNCH_ERROR;
+        }
+        return SUNNY_GENEIG_OK;
     }
     const long long fit = (long long)(kNoAllocScratchBytes / slot);
     const int slots = (int)(fit < 2LL * d->sms ? fit : 2LL * d->sms);

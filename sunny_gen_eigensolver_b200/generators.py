@@ -62,6 +62,20 @@ def baseline_problems(n: int, batch: int, seed: int, kappa: float = DEFAULT_KAPP
     return H, S
 
 
+def spawned_problems(n: int, batch: int, seed: int, kappa: float = DEFAULT_KAPPA):
+    """Baseline distribution with one independent substream per problem:
+    problem b is drawn from PCG64(SeedSequence(seed).spawn(batch)[b]), so any
+    problem regenerates on its own. The parity set of 256 problems at N=54 is
+    spawned_problems(54, 256, 20261203)."""
+    H = np.empty((batch, n, n), dtype=np.complex128)
+    S = np.empty((batch, n, n), dtype=np.complex128)
+    for b, ss in enumerate(np.random.SeedSequence(seed).spawn(batch)):
+        rng = np.random.Generator(np.random.PCG64(ss))
+        H[b] = _hermitian_bdg_np(rng, n, 1)[0]
+        S[b] = _spd_haar_np(rng, n, 1, kappa)[0]
+    return H, S
+
+
 def sigma_metric_problems(n: int, batch: int, seed: int):
     """Sunny call pattern: H = diag(I_m, -I_m) (indefinite), S = PD BdG matrix."""
     rng = np.random.Generator(np.random.PCG64(seed))

@@ -9,7 +9,7 @@ before recording, per fixture, the SHA-256 of H and S (column-major bytes,
 as in the file), all eigenvalues W, and the eigenvectors U of the first two
 matrices for N in {16, 54}.
 
-Run (needs the reference checkout):  python tests/golden/make_golden.py [REF_ROOT]
+Run (needs a checkout of the reference):  python tests/golden/make_golden.py REF_ROOT
 """
 from __future__ import annotations
 
@@ -30,7 +30,7 @@ def colmajor_bytes(M):
     return np.ascontiguousarray(M.transpose(0, 2, 1)).tobytes()
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str) -> None:
     data = Path(ref_root) / "tests" / "data"
     out = {}
     names = []
@@ -54,4 +54,6 @@ def main(ref_root: str = "/root/reference") -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py REF_ROOT  (root of a reference checkout)")
+    main(sys.argv[1])

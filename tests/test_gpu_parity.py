@@ -292,3 +292,44 @@ def test_create_config_explicit_and_rejected(cuda):
                     ({"slots_per_sm": 3}, "slots_per_sm")):
         with pytest.raises(RuntimeError, match=msg):
             Solver(100, **kw)
+
+
+def test_graph_replay_ordered_with_launches_on_other_streams(cuda):
+    """An l2-slot handle (scratch slots shared by all its launches) used both
+    by a captured CUDA graph replayed on one stream and by normal launches on
+    another stream: the replays and the launches must not overlap on the
+    device, so every result equals the one-at-a-time result bit for bit."""
+    import torch
+    from sunny_gen_eigensolver_b200 import Solver, to_colmajor
+    n, batch = 72, 96
+    HA, SA = generators.baseline_problems(n, batch, seed=71)
+    HB, SB = generators.baseline_problems(n, batch, seed=72)
+    dev = torch.device("cuda")
+    bufs = []
+    for H, S in ((HA, SA), (HB, SB)):
+        bufs.append((to_colmajor(torch.from_numpy(H).to(dev)), to_colmajor(torch.from_numpy(S).to(dev)),
+                     torch.zeros((batch, n), dtype=torch.float64, device=dev),
+                     torch.zeros((batch, n, n), dtype=torch.complex128, device=dev),
+                     torch.zeros((batch,), dtype=torch.int32, device=dev)))
+    with Solver(n) as s:
+        assert s.regime == "l2-slot"
+        ref = []
+        for Hc, Sc, W, U, info in bufs:
+            s.launch(Hc, Sc, W, U, info)
+            torch.cuda.synchronize()
+            ref.append((W.clone(), U.clone(), info.clone()))
+            W.zero_(); U.zero_(); info.fill_(-7)
+        s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        g = torch.cuda.CUDAGraph()
+        s1.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.graph(g, stream=s1):
+            s.launch(*bufs[0], stream=s1)
+        for _ in range(3):
+            with torch.cuda.stream(s1):
+                g.replay()
+            s.launch(*bufs[1], stream=s2)
+            s.launch(*bufs[1], stream=s2)
+        torch.cuda.synchronize()
+        for (Hc, Sc, W, U, info), (Wr, Ur, ir) in zip(bufs, ref):
+            assert torch.equal(info, ir) and torch.equal(W, Wr) and torch.equal(U, Ur)
+        del g

@@ -1,8 +1,10 @@
 """sunny_geneig_launch_noalloc: the solve for callers that cannot allocate
 device memory (code inside another framework's memory pool or under a
 no-allocation policy, plugins whose host forbids cudaMalloc, graph-replay
-setups that must not touch the allocator). It takes no handle and uses a
-fixed device array built into the library as its scratch.
+setups that must not touch the allocator). It takes no handle; up to n = 60
+it runs the shared-memory kernel, which needs no scratch, and above that it
+uses a fixed device array built into the library as its scratch (n = 54 and
+n = 96 below cover both).
 
 Checked here through the C ABI against the regular entry point
 (sunny_geneig_create_ex + sunny_geneig_launch) on the same inputs, on two
