@@ -29,7 +29,6 @@ namespace {
 
 constexpr int kNT = 256;
 constexpr int kG = 4;
-constexpr int kNG = kNT / kG;
 
 struct CtaArgs {
     const double2* __restrict__ H;
@@ -158,7 +157,6 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tr = tid >> 4, tc = tid & 15;
     const int g = tid >> 2, q = tid & 3;
-    const unsigned gmask = 0xFu << (lane & ~3);
     const size_t nn = (size_t)n * n;
 
     phase_start();
@@ -327,24 +325,44 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         }
 
         if (!code) {
-            // ---- a5a: Householder tridiagonalisation of C (lower). Reflector k:
-            // I - tau_k v v^H on rows k+1.., v[k+1] = 1, v[k+2..] kept in A's
-            // strict upper triangle (row k), tau_k in v.tau. Look-ahead: during
-            // the rank-2 update of step k, warp 0 updates column k+1 first and
-            // computes reflector k+1 (into the other vector buffer) while warps
-            // 1-7 update the rest, so each step needs two barriers.
-            auto reflect = [&](int k, double2* vbuf) {   // warp 0
-                const double2* bk = B + (size_t)k * ld;
+            // ---- a5a: Householder tridiagonalisation of C (lower, the zhetd2 /
+            // zlarfg conventions: reflector k is I - tau_k v v^H on rows k+1..,
+            // v[k+1] = 1, T real). C lives in registers: thread (tr, tc) holds
+            // C(i, j) for i = tr + 16 a, j = tc + 16 b, so a step moves only
+            // vectors through shared memory. Step k:
+            //   P  every warp forms reflector k from column k (colb; C's own
+            //      column 0 in B for k = 0) redundantly, so that no barrier is
+            //      needed; p = tau C22 v from register partial rows reduced
+            //      over the 16 lanes that share them; per-warp partials of p^H v
+            //   -- barrier
+            //   U  w = p + alpha2 v with alpha2 = -tau/2 (p^H v), C22 -= v w^H +
+            //      w v^H in registers; the owners of column k+1 publish it
+            //   -- barrier
+            // Blocks of 16 rows (columns) that lie wholly above (left of) the
+            // active part are skipped. v[k+2..] is also kept in A's strict upper
+            // triangle (row k) for the back-transform, tau_k in v.tau.
+            constexpr int NB = (NMAX + 15) / 16;
+            double2 cr[NB][NB];
+#pragma unroll
+            for (int a_ = 0; a_ < NB; ++a_)
+#pragma unroll
+                for (int b_ = 0; b_ < NB; ++b_) {
+                    const int i = tr + 16 * a_, j = tc + 16 * b_;
+                    cr[a_][b_] = (i < n && j < n) ? B[i + (size_t)j * ld] : c2(0.0, 0.0);
+                }
+            double2* vbuf = v.vb;    // v of the current step (rows > k)
+            double2* colb = v.vb2;   // column k + 1 of the updated matrix (rows > k)
+            for (int k = 0; k < n - 1; ++k) {
+                const double2* col = (k == 0) ? B : colb;
+                const int kb = (k + 1) >> 4;   // first block with an active row
+                // -- P: reflector k (zlarfg), identical in every warp
                 double ss = 0.0;
-                for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = bk[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = col[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
                 ss = warp_sum(ss);
-                const double2 alpha = bk[k + 1];
-                double2 taui, scal = c2(0.0, 0.0);
-                double beta;
-                if (ss == 0.0 && alpha.y == 0.0) {
-                    taui = c2(0.0, 0.0);
-                    beta = alpha.x;
-                } else {
+                const double2 alpha = col[k + 1];
+                double2 taui = c2(0.0, 0.0), scal = c2(0.0, 0.0);
+                double beta = alpha.x;
+                if (!(ss == 0.0 && alpha.y == 0.0)) {
                     beta = -copysign(sqrt(fma(alpha.x, alpha.x, fma(alpha.y, alpha.y, ss))), alpha.x);
                     const double rb = fast_rcp(beta);
                     taui = c2((beta - alpha.x) * rb, -alpha.y * rb);
@@ -352,86 +370,91 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                     const double inv = fast_rcp(fma(z.x, z.x, z.y * z.y));
                     scal = c2(z.x * inv, -z.y * inv);
                 }
-                for (int i = k + 2 + lane; i < n; i += 32) {
-                    const double2 vi = cmul(bk[i], scal);
-                    vbuf[i] = vi;
-                    A[k + (size_t)i * ld] = vi;
-                }
-                if (lane == 0) {
-                    vbuf[k + 1] = c2(1.0, 0.0);
-                    v.tau[k] = taui;
-                    v.d[k] = bk[k].x;
-                    v.e[k] = beta;
-                }
-            };
-            if (n >= 2 && warp == 0) reflect(0, v.vb);
-            __syncthreads();
-            for (int k = 0; k < n - 1; ++k) {
-                double2* vk = (k & 1) ? v.vb2 : v.vb;
-                double2* vn = (k & 1) ? v.vb : v.vb2;
-                const double2 taui = v.tau[k];
                 const bool has = !(taui.x == 0.0 && taui.y == 0.0);
-                if (has) {
-                    // p = tau A22 v: four lanes per row; per-warp partial of p^H v
-                    double2 dotp = c2(0.0, 0.0);
-                    for (int i = k + 1 + g; i < n; i += kNG) {
-                        double2 acc = c2(0.0, 0.0);
-                        for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], vk[j]);
-                        acc = group_sum2<kG>(gmask, acc);
-                        const double2 pi = cmul(taui, acc);
-                        if (q == 0) { v.pb[i] = pi; dotp = cfmac(dotp, pi, vk[i]); }
+                if (warp == (k & 7)) {
+                    for (int i = k + 2 + lane; i < n; i += 32) {
+                        const double2 vi = cmul(col[i], scal);
+                        vbuf[i] = vi;
+                        A[k + (size_t)i * ld] = vi;
                     }
-                    dotp = warp_sum2(dotp);
-                    if (lane == 0) v.wred[warp] = dotp;
-                    __syncthreads();
+                    if (lane == 0) {
+                        vbuf[k + 1] = c2(1.0, 0.0);
+                        v.tau[k] = taui;
+                        v.d[k] = col[k].x;
+                        v.e[k] = beta;
+                    }
                 }
-                // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v)
-                double2 alpha2 = c2(0.0, 0.0);
+                if (has) {
+                    double2 vc[NB];
+#pragma unroll
+                    for (int b_ = 0; b_ < NB; ++b_) {
+                        const int j = tc + 16 * b_;
+                        vc[b_] = (j == k + 1) ? c2(1.0, 0.0) : (j > k + 1 && j < n) ? cmul(col[j], scal) : c2(0.0, 0.0);
+                    }
+                    double2 dp = c2(0.0, 0.0);
+#pragma unroll
+                    for (int a_ = 0; a_ < NB; ++a_) {
+                        if (a_ < kb) continue;
+                        double2 pr = c2(0.0, 0.0);
+#pragma unroll
+                        for (int b_ = 0; b_ < NB; ++b_)
+                            if (b_ >= kb) pr = cfma(pr, cr[a_][b_], vc[b_]);
+                        pr = group_sum2<16>(0xffffffffu, pr);
+                        const int i = tr + 16 * a_;
+                        const double2 pi = (i > k && i < n) ? cmul(taui, pr) : c2(0.0, 0.0);
+                        if (tc == a_ && i < n) v.pb[i] = pi;
+                        if (tc == 0 && i > k && i < n) {
+                            const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : cmul(col[i], scal);
+                            dp = cfmac(dp, pi, vi);
+                        }
+                    }
+                    dp.x += __shfl_xor_sync(0xffffffffu, dp.x, 16);
+                    dp.y += __shfl_xor_sync(0xffffffffu, dp.y, 16);
+                    if (lane == 0) v.wred[warp] = dp;
+                }
+                __syncthreads();
+                // -- U: rank-2 update in registers
                 if (has) {
                     double2 dot = c2(0.0, 0.0);
 #pragma unroll
                     for (int w = 0; w < kNT / 32; ++w) dot = cadd(dot, v.wred[w]);
-                    alpha2 = cscale(cmul(taui, dot), -0.5);
-                }
-                if (warp == 0) {
-                    if (has) {
-                        const int j = k + 1;
-                        const double2 vj = vk[j];
-                        const double2 wj = cfma(v.pb[j], alpha2, vj);
-                        for (int i = j + lane; i < n; i += 32) {
-                            const double2 vi = vk[i];
-                            const double2 wi = cfma(v.pb[i], alpha2, vi);
-                            double2* p = B + i + (size_t)j * ld;
-                            *p = cfms_bc(cfms_bc(*p, vi, wj), wi, vj);
-                        }
-                        __syncwarp();
+                    const double2 alpha2 = cscale(cmul(taui, dot), -0.5);
+                    double2 vr[NB], wr[NB];
+#pragma unroll
+                    for (int a_ = 0; a_ < NB; ++a_) {
+                        const int i = tr + 16 * a_;
+                        const bool act = i > k && i < n;
+                        vr[a_] = act ? vbuf[i] : c2(0.0, 0.0);
+                        wr[a_] = act ? cfma(v.pb[i], alpha2, vr[a_]) : c2(0.0, 0.0);
                     }
-                    if (k + 1 < n - 1) reflect(k + 1, vn);
-                } else if (has) {
-                    // group g - 8 of warps 1-7 takes rows k+1+(g-8), +56, ...;
-                    // its lanes take columns j = k+2+q step 4 (column k+1 is warp 0's)
-                    for (int i = k + 1 + (g - 8); i < n; i += kNG - 8) {
-                        const double2 vi = vk[i];
-                        const double2 wi = cfma(v.pb[i], alpha2, vi);
-                        double2* bi = B + i;
-                        int j = k + 2 + q;
-                        for (; j + 4 < n; j += 8) {
-                            const double2 x0 = bi[(size_t)j * ld], x1 = bi[(size_t)(j + 4) * ld];
-                            const double2 v0 = vk[j], v1 = vk[j + 4];
-                            const double2 w0 = cfma(v.pb[j], alpha2, v0), w1 = cfma(v.pb[j + 4], alpha2, v1);
-                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(x0, vi, w0), wi, v0);
-                            bi[(size_t)(j + 4) * ld] = cfms_bc(cfms_bc(x1, vi, w1), wi, v1);
-                        }
-                        if (j < n) {
-                            const double2 v0 = vk[j];
-                            const double2 w0 = cfma(v.pb[j], alpha2, v0);
-                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(bi[(size_t)j * ld], vi, w0), wi, v0);
-                        }
+#pragma unroll
+                    for (int b_ = 0; b_ < NB; ++b_) {
+                        if (b_ < kb) continue;
+                        const int j = tc + 16 * b_;
+                        const bool act = j > k && j < n;
+                        const double2 vj = act ? vbuf[j] : c2(0.0, 0.0);
+                        const double2 wj = act ? cfma(v.pb[j], alpha2, vj) : c2(0.0, 0.0);
+#pragma unroll
+                        for (int a_ = 0; a_ < NB; ++a_)
+                            if (a_ >= kb) cr[a_][b_] = cfms_bc(cfms_bc(cr[a_][b_], vr[a_], wj), wr[a_], vj);
+                    }
+                }
+                // publish column k + 1 (rows > k) for the next step
+                if (tc == ((k + 1) & 15)) {
+                    const int bsel = (k + 1) >> 4;
+#pragma unroll
+                    for (int a_ = 0; a_ < NB; ++a_) {
+                        const int i = tr + 16 * a_;
+                        double2 x = cr[a_][0];
+#pragma unroll
+                        for (int b_ = 1; b_ < NB; ++b_)
+                            if (b_ == bsel) x = cr[a_][b_];
+                        if (i > k && i < n) colb[i] = x;
                     }
                 }
                 __syncthreads();
             }
-            if (tid == 0) v.d[n - 1] = B[(n - 1) + (size_t)(n - 1) * ld].x;
+            if (tid == 0) v.d[n - 1] = (n == 1) ? B[0].x : colb[n - 1].x;
             __syncthreads();
             phase_mark(4);
             // ---- a5b: divide and conquer; Z (real) and its workspace in B
@@ -472,54 +495,174 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             v.rank[j] = r;
             Wb[r] = v.dcd[j];
         }
-        // ---- a5c: V = Q Z, one column per four-lane group, in registers.
-        // Reflectors are applied in blocks of 16 (k from 16c+15 down to 16c);
-        // rows below 16c are untouched by a block, so the loops over a lane's
-        // rows start at the block (compile-time bounds), predicated only
-        // inside the diagonal block.
+        // ---- a5c: V = Q Z with Q = H_0 H_1 ... H_{n-2} in compact-WY blocks of
+        // 16 reflectors on the FP64 tensor cores. Block c (reflectors 16c ..,
+        // m_c of them) is Q_c = I - Y_c T_c Y_c^H (the zlarft forward,
+        // columnwise T: T(l, l) = tau_l, T(0:l, l) = -tau_l T(0:l, 0:l) Y^H y_l),
+        // and V = Q_0 (Q_1 (... Q_last Z)). Steps:
+        //   1. G_c = Y_c^H Y_c (MMA tiles, upper 8x8 tiles), packed into the
+        //      vector area (free from here on); Z (real) into registers.
+        //   2. V = Z as complex in B; T_c by its column recurrence, one warp per
+        //      block, written over G_c column by column.
+        //   3. warp p owns columns [8p, 8p+8) of V and applies the blocks, last
+        //      first, with no CTA barrier: W1 = Y_c^H V_p, W2 = T_c W1,
+        //      V_p -= Y_c W2, the 8-column intermediates passed between MMA
+        //      fragment layouts by shuffles.
         {
-            double2 x[R];
-            const double* Z = reinterpret_cast<const double*>(B);
-            const int j = g;
+            const int nref = n - 1;                      // reflectors 0 .. n-2
+            const int nblk = (nref + 15) >> 4;
+            double2* tpk = v.vb;                         // packed upper T_c (G_c before)
+            auto tidx = [](int c, int l, int i) { return 136 * c + ((i * (i + 1)) >> 1) + l; };
+            // Y_c(r, l): reflector k = 16c + l, v_k[k+1] = 1, v_k[r] in A's row k
+            auto yv = [&](int c, int r, int l) -> double2 {
+                const int k = 16 * c + l;
+                if (k >= nref || r <= k || r >= n) return c2(0.0, 0.0);
+                return (r == k + 1) ? c2(1.0, 0.0) : A[k + (size_t)r * ld];
+            };
+            // 1. Gram blocks: tiles (c, hr, hc) with hr <= hc, dealt to the warps
+            for (int t = warp; t < 3 * nblk; t += kNT / 32) {
+                const int c = t / 3, hh = t - 3 * c;
+                const int hr = hh == 2 ? 1 : 0, hc = hh == 0 ? 0 : 1;
+                double gr[2] = {0.0, 0.0}, gi[2] = {0.0, 0.0};
+                const int la = 8 * hr + (lane >> 2), lb = 8 * hc + (lane >> 2);
+                for (int k0 = 16 * c; k0 < n; k0 += 4) {
+                    const int r = k0 + (lane & 3);
+                    const double2 ya = yv(c, r, la);   // A(l, r) = conj(Y(r, l))
+                    const double2 yb = yv(c, r, lb);   // B(r, l') = Y(r, l')
+                    mma884(gr[0], gr[1], ya.x, yb.x);
+                    mma884(gr[0], gr[1], ya.y, yb.y);
+                    mma884(gi[0], gi[1], ya.x, yb.y);
+                    mma884(gi[0], gi[1], -ya.y, yb.x);
+                }
+                const int l = 8 * hr + (lane >> 2);
 #pragma unroll
-            for (int t = 0; t < R; ++t) {
-                const int i = q + kG * t;
-                x[t] = c2((j < n && i < n) ? Z[i + (size_t)j * ld] : 0.0, 0.0);
+                for (int e2 = 0; e2 < 2; ++e2) {
+                    const int i = 8 * hc + 2 * (lane & 3) + e2;
+                    if (l < i && 16 * c + i < nref) tpk[tidx(c, l, i)] = c2(gr[e2], gi[e2]);
+                }
             }
-            __syncthreads();   // B is free from here on
-            if (j < n) {
+            // Z (real) into registers, then V = Z as complex in place
+            constexpr int ZR = (NMAX * NMAX + kNT - 1) / kNT;
+            double zr[ZR];
+            const double* Z = reinterpret_cast<const double*>(B);
 #pragma unroll
-                for (int c = (NMAX + 15) / 16 - 1; c >= 0; --c) {
-                    const int khi = min(16 * c + 15, n - 2);
-                    for (int k = khi; k >= 16 * c; --k) {
-                        const double2 tk = v.tau[k];
-                        if (tk.x == 0.0 && tk.y == 0.0) continue;
-                        const double2* vk = A + k;   // v_k[i] = vk[i*ld] (i >= k+2), v_k[k+1] = 1
-                        double2 s0 = c2(0.0, 0.0), s1 = c2(0.0, 0.0);
+            for (int u = 0; u < ZR; ++u) {
+                const int idx = tid + kNT * u, j = idx / n, i = idx - j * n;
+                zr[u] = (idx < n * n) ? Z[i + (size_t)j * ld] : 0.0;
+            }
+            __syncthreads();
 #pragma unroll
-                        for (int t = 4 * c; t < R; ++t) {
-                            const int i = q + kG * t;
-                            if (i > k && i < n) {
-                                const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
-                                if (t & 1) s1 = cfmac(s1, vi, x[t]); else s0 = cfmac(s0, vi, x[t]);
+            for (int u = 0; u < ZR; ++u) {
+                const int idx = tid + kNT * u, j = idx / n, i = idx - j * n;
+                if (idx < n * n) B[i + (size_t)j * ld] = c2(zr[u], 0.0);
+            }
+            // 2. T_c: lane l of warp c holds row l of T_c; column i needs
+            // T(l, m < i) and G(m, i) (l <= m < i); every lane reads column i of
+            // G before any lane overwrites it with column i of T.
+            if (warp < nblk) {
+                const int c = warp, l = lane;
+                const int mc = min(16, nref - 16 * c);
+                double2 trow[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    trow[i] = c2(0.0, 0.0);
+                    if (i < mc && l < 16 && l <= i) {
+                        const double2 ti = v.tau[16 * c + i];
+                        if (l == i) {
+                            trow[i] = ti;
+                        } else {
+                            double2 s0 = c2(0.0, 0.0), s1 = c2(0.0, 0.0);
+#pragma unroll
+                            for (int m = 0; m < i; ++m) {
+                                if (m < l) continue;
+                                const double2 gm = tpk[tidx(c, m, i)];
+                                if (m & 1) s1 = cfma(s1, trow[m], gm); else s0 = cfma(s0, trow[m], gm);
                             }
-                        }
-                        double2 s = group_sum2<kG>(gmask, cadd(s0, s1));
-                        const double2 ts = cmul(tk, s);
-#pragma unroll
-                        for (int t = 4 * c; t < R; ++t) {
-                            const int i = q + kG * t;
-                            if (i > k && i < n) {
-                                const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : vk[(size_t)i * ld];
-                                x[t] = cfms(x[t], ts, vi);
-                            }
+                            trow[i] = cscale(cmul(ti, cadd(s0, s1)), -1.0);
                         }
                     }
+                    __syncwarp();
+                    if (i < mc && l < 16 && l <= i) tpk[tidx(c, l, i)] = trow[i];
+                    __syncwarp();
                 }
+            }
+            __syncthreads();
+            // 3. per-warp panels: columns [8p, 8p+8), p = warp (n <= 64)
+            const int p = warp;
+            if (8 * p < n) {
+                const int jb = 8 * p + (lane >> 2);   // B-fragment column of this lane
+                // W (16 x 8, accumulator layout: rows 8h + lane/4, columns
+                // 2(lane%4) + e) -> B-fragment layout for k-step s: element
+                // (4s + lane%4, lane/4), returned as (re, im) scaled by `sgn`
+                auto to_bfrag = [&](const double (&wr)[2][2], const double (&wi)[2][2], int s, double sgn,
+                                    double& br, double& bi) {
+                    const int src = 16 * (s & 1) + 4 * (lane & 3) + (lane >> 3);
+                    const int h = s >> 1, e2 = (lane >> 2) & 1;
+                    const double r0 = __shfl_sync(0xffffffffu, wr[h][0], src);
+                    const double r1 = __shfl_sync(0xffffffffu, wr[h][1], src);
+                    const double i0 = __shfl_sync(0xffffffffu, wi[h][0], src);
+                    const double i1 = __shfl_sync(0xffffffffu, wi[h][1], src);
+                    br = sgn * (e2 ? r1 : r0);
+                    bi = sgn * (e2 ? i1 : i0);
+                };
+                for (int c = nblk - 1; c >= 0; --c) {
+                    // W1 = Y_c^H V_p  (16 x 8, K = rows 16c .. n-1)
+                    double w1r[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, w1i[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+                    for (int k0 = 16 * c; k0 < n; k0 += 4) {
+                        const int r = k0 + (lane & 3);
+                        const double2 vb_ = (r < n && jb < n) ? B[r + (size_t)jb * ld] : c2(0.0, 0.0);
 #pragma unroll
-                for (int t = 0; t < R; ++t) {
-                    const int i = q + kG * t;
-                    if (i < n) B[i + (size_t)j * ld] = x[t];
+                        for (int h = 0; h < 2; ++h) {
+                            const double2 ya = yv(c, r, 8 * h + (lane >> 2));
+                            mma884(w1r[h][0], w1r[h][1], ya.x, vb_.x);
+                            mma884(w1r[h][0], w1r[h][1], ya.y, vb_.y);
+                            mma884(w1i[h][0], w1i[h][1], ya.x, vb_.y);
+                            mma884(w1i[h][0], w1i[h][1], -ya.y, vb_.x);
+                        }
+                    }
+                    // W2 = T_c W1 (T upper, K = 16), negated for the update
+                    double w2r[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, w2i[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) {
+                        double br, bi;
+                        to_bfrag(w1r, w1i, s, -1.0, br, bi);
+                        const int kk = 4 * s + (lane & 3);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int l = 8 * h + (lane >> 2);
+                            const double2 ta = (l <= kk && 16 * c + kk < nref) ? tpk[tidx(c, l, kk)] : c2(0.0, 0.0);
+                            mma884(w2r[h][0], w2r[h][1], ta.x, br);
+                            mma884(w2r[h][0], w2r[h][1], -ta.y, bi);
+                            mma884(w2i[h][0], w2i[h][1], ta.x, bi);
+                            mma884(w2i[h][0], w2i[h][1], ta.y, br);
+                        }
+                    }
+                    // V_p += Y_c (-W2) on row tiles from 2c (rows < 16c + 1 get 0)
+                    double bfr[4], bfi[4];
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) to_bfrag(w2r, w2i, s, 1.0, bfr[s], bfi[s]);
+                    const int j0 = 8 * p + 2 * (lane & 3);
+                    for (int t = 2 * c; 8 * t < n; ++t) {
+                        const int r = 8 * t + (lane >> 2);
+                        double ar[2], ai[2];
+#pragma unroll
+                        for (int e2 = 0; e2 < 2; ++e2) {
+                            const double2 x = (r < n && j0 + e2 < n) ? B[r + (size_t)(j0 + e2) * ld] : c2(0.0, 0.0);
+                            ar[e2] = x.x; ai[e2] = x.y;
+                        }
+#pragma unroll
+                        for (int s = 0; s < 4; ++s) {
+                            const double2 ya = yv(c, r, 4 * s + (lane & 3));   // A(r, l) = Y(r, l)
+                            mma884(ar[0], ar[1], ya.x, bfr[s]);
+                            mma884(ar[0], ar[1], -ya.y, bfi[s]);
+                            mma884(ai[0], ai[1], ya.x, bfi[s]);
+                            mma884(ai[0], ai[1], ya.y, bfr[s]);
+                        }
+#pragma unroll
+                        for (int e2 = 0; e2 < 2; ++e2)
+                            if (r < n && j0 + e2 < n) B[r + (size_t)(j0 + e2) * ld] = c2(ar[e2], ai[e2]);
+                    }
+                    __syncwarp();
                 }
             }
         }
