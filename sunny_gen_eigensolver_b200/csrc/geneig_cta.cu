@@ -759,6 +759,7 @@ extern "C" int sunny_geneig_phase_cycles(unsigned long long* out, int count, int
         static const unsigned long long zeros[sgeig::kPhaseSlots] = {};
         e = cudaMemcpyToSymbol(sgeig::g_phase_cycles, zeros, sizeof(zeros));
     }
+    if (e == cudaSuccess && out && count > 0) e = sgeig::tiled_phase_cycles(out, count, reset != 0);
     return e == cudaSuccess ? 0 : -1;
 }
 #pragma GCC visibility pop

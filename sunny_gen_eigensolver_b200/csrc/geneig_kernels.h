@@ -87,6 +87,11 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage,
                          int* info, long long batch, void* scratch,
                          cudaStream_t stream, bool sigma = false);
 
+#ifdef SGEIG_PHASE_TIMERS
+// Profiling builds only: adds the tiled kernel's phase counters into out.
+cudaError_t tiled_phase_cycles(unsigned long long* out, int count, bool reset);
+#endif
+
 // Thread-local last-error text of the C ABI (defined in c_api.cpp), for
 // entry points implemented in other translation units.
 void api_set_error(const std::string& msg);

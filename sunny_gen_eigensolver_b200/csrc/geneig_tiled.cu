@@ -265,6 +265,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
     const size_t nn = (size_t)n * n;
     const double2 zero = c2(0.0, 0.0);
 
+    phase_start();
     for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) {
         const double2* Hb = a.H + (size_t)b * nn;
         const double2* Sb = a.S + (size_t)b * nn;
@@ -272,6 +273,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
         double2* Ub = a.U + (size_t)b * nn;
 
         __syncthreads();  // previous pencil fully consumed
+        phase_mark(24);
         // ---- a1: S (lower triangle and diagonal) -> M0
         for (int idx = tid; idx < (int)nn; idx += kNT) {
             const int j = idx / n, i = idx - j * n;
@@ -279,6 +281,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
         }
         if (tid < 8) v.ctl[tid] = 0;
         __syncthreads();
+        phase_mark(16);
 
         // ---- a2: blocked Cholesky (lower). The pivot test is the same as
         // potrf's (not > 0, NaN included), taken in column order.
@@ -326,6 +329,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
             __syncthreads();
         }
         int code = fail ? n + fail : 0;   // zhegv: info = n + order of the failing minor
+        phase_mark(17);
 
         if (!code && a.stage >= 2) {
             // ---- a3: X = L^-1 -> M1, block row r0..re at a time
@@ -365,6 +369,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
                 }
                 __syncthreads();
             }
+            phase_mark(18);
         }
 
         if (!code && a.stage == 1) {
@@ -419,6 +424,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
                 });
             }
             __syncthreads();
+            phase_mark(19);
         }
 
         if (!code && a.stage == 2) {
@@ -730,6 +736,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
                     if (n == 1) v.tau[0] = zero;
                 }
                 __syncthreads();
+                phase_mark(20);
 
                 // ---- a5b: divide and conquer on T: Z in M2 (real), its merge
                 // workspace after it, merge products through Zo
@@ -761,6 +768,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
                     }
                 }
                 __syncthreads();
+                phase_mark(21);
             }
 
             if (code) break;
@@ -1004,6 +1012,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
 
             break;
         }
+        phase_mark(22);
         if (code) {
             const double qnan = __longlong_as_double(0x7ff8000000000000LL);
             for (int idx = tid; idx < (int)nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
@@ -1026,6 +1035,7 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
             z16_store(acc, i0, j0, [&](int i, int j, double2 x) { if (i < n && j < n) M2[i + (size_t)j * ld] = x; });
         }
         __syncthreads();
+        phase_mark(23);
         for (int idx = tid; idx < (int)nn; idx += kNT) {
             const int j = idx / n, i = idx - j * n;
             Ub[i + (size_t)(use32 ? v.rank[j] : j) * n] = M2[i + (size_t)j * ld];
@@ -1068,3 +1078,20 @@ cudaError_t tiled_launch(int n, int slots, size_t smem, int stage, const void* H
 }
 
 }  // namespace sgeig
+
+#ifdef SGEIG_PHASE_TIMERS
+namespace sgeig {
+// Profiling builds only: this translation unit's phase counters (the tiled
+// kernel's marks), added into `out` by sunny_geneig_phase_cycles.
+cudaError_t tiled_phase_cycles(unsigned long long* out, int count, bool reset) {
+    unsigned long long mine[kPhaseSlots] = {};
+    cudaError_t e = cudaMemcpyFromSymbol(mine, g_phase_cycles, sizeof(mine));
+    for (int i = 0; e == cudaSuccess && i < count && i < kPhaseSlots; ++i) out[i] += mine[i];
+    if (e == cudaSuccess && reset) {
+        static const unsigned long long zeros[kPhaseSlots] = {};
+        e = cudaMemcpyToSymbol(g_phase_cycles, zeros, sizeof(zeros));
+    }
+    return e;
+}
+}  // namespace sgeig
+#endif

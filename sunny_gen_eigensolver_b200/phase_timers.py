@@ -1,9 +1,10 @@
-"""Per-phase cycle split of the smem-cta kernel (profiling aid).
+"""Per-phase cycle split of the solver kernels (profiling aid).
 
 Builds (if needed) and loads the profiling variant of the library,
-lib/libsunny_geneig_timers.so, whose kernels carry clock64 marks after their
-CTA barriers (phase_mark in csrc/geneig_common.cuh), runs one solve of a
-seeded batch, and prints the CTA cycles per solve spent in each phase.
+lib/libsunny_geneig_timers.so, whose kernels (smem-cta and l2-slot) carry
+clock64 marks after their CTA barriers (phase_mark in
+csrc/geneig_common.cuh), runs a seeded batch through the size's default
+kernel, and prints the CTA cycles per solve spent in each phase.
 
   python -m sunny_gen_eigensolver_b200.phase_timers [--n 54] [--batch 8192] [--reps 3]
 
@@ -27,6 +28,11 @@ PHASES = {
     6: "a5c rank + back-transform V = Q Z", 7: "a6 U = X^H V", 8: "a7 store U (+ loop barrier)",
     10: "D&C scale + leaves", 11: "D&C deflation (phase A)", 12: "D&C secular roots (phase B)",
     13: "D&C Loewner z (phase C)", 14: "D&C rank-one vectors (phase D)", 15: "D&C merge GEMMs (phase E)",
+    # l2-slot (tiled) kernel
+    16: "tiled a1 load S", 17: "tiled a2 blocked Cholesky", 18: "tiled a3 X = L^-1",
+    19: "tiled a4 T = H X^H, C = X T", 20: "tiled a5a Householder", 21: "tiled a5b D&C tail + rank",
+    22: "tiled a5c WY back-transform (+ mixed refinement)", 23: "tiled a6 U = X^H V",
+    24: "tiled a7 store U (+ loop barrier)",
 }
 
 
