@@ -14,12 +14,19 @@ time (Poisson in the benchmark); the engine
   on the device),
 * releases a request's budget as soon as its completion event fires and
   admits the next ones,
+* survives a failed start (the executor could not allocate the request's
+  buffers): the request goes back to the head of the queue, the engine
+  admits nothing more until an in-flight request has finished and freed
+  memory, then retries; a request that cannot start even with nothing else
+  in flight fails with the error as its result,
 * records per-request latency (arrival to completion) and reports p50/p99
   latency, solves/s and queue statistics.
 
-The GPU work goes through an executor (`DeviceExecutor`: one Solver per N,
-a pool of CUDA streams, the C ABI launch); `SimExecutor` replaces it with a
-clock model so that the admission logic can be tested without a GPU.
+The GPU work goes through an executor (`DeviceExecutor`: per N a small pool
+of Solver handles, so that requests of the same N can overlap on the device,
+in the plain FP64 or the mixed-precision form, a pool of CUDA streams, the C
+ABI launch); `SimExecutor` replaces it with a clock model so that the
+admission logic can be tested without a GPU.
 """
 from __future__ import annotations
 
@@ -67,6 +74,8 @@ class ServeStats:
     max_waiting: int = 0
     max_in_flight: int = 0
     peak_budget_bytes: int = 0
+    start_failures: int = 0        # starts the executor could not allocate (retried)
+    failed_requests: int = 0       # requests that could not start at all
     by_n: Dict[int, int] = field(default_factory=dict)
 
     @property
@@ -119,6 +128,7 @@ class ServingEngine:
         waiting: List[Request] = []
         in_flight: List[tuple] = []          # (request, handle)
         used = 0
+        blocked = 0                          # in-flight count at a failed start (0: admitting)
         st = ServeStats()
         clock = self.ex.clock
         t0 = clock()
@@ -146,16 +156,34 @@ class ServingEngine:
                 else:
                     still.append((r, h))
             in_flight = still
-            # admit in arrival order while a slot and the budget allow
-            while waiting and len(in_flight) < self.slots:
+            # admit in arrival order while a slot and the budget allow; after a
+            # failed start admit nothing until an in-flight request finishes
+            if blocked and len(in_flight) < blocked:
+                blocked = 0
+            while waiting and len(in_flight) < self.slots and not blocked:
                 r = waiting[0]
                 need = request_bytes(r.n, r.q)
                 if used + need > self.budget:
                     break
+                try:
+                    h = self.ex.start(r)
+                except (MemoryError, RuntimeError) as err:
+                    st.start_failures += 1
+                    if in_flight:
+                        blocked = len(in_flight)      # retry once one of these has finished
+                        break
+                    waiting.pop(0)                    # nothing else holds memory: give up on it
+                    r.admitted = r.done = clock() - t0
+                    st.failed_requests += 1
+                    if self.consume is not None:
+                        self.consume(r, err)
+                    else:
+                        r.result = err
+                    continue
                 waiting.pop(0)
                 used += need
                 r.admitted = clock() - t0
-                in_flight.append((r, self.ex.start(r)))
+                in_flight.append((r, h))
                 st.peak_budget_bytes = max(st.peak_budget_bytes, used)
             st.max_in_flight = max(st.max_in_flight, len(in_flight))
             next_arrival = t0 + pending[i].arrival if (i < len(pending) and realtime) else None
@@ -207,15 +235,22 @@ class DeviceExecutor:
     problems (a stand-in for Sunny's on-device assembly of H and S)."""
 
     def __init__(self, device: int = 0, slots: int = 8, pool_size: int = 256, kappa: float = 100.0,
-                 poll_sleep_s: float = 50e-6):
+                 poll_sleep_s: float = 50e-6, kernel: str = "unified", handles_per_n: int = 2):
+        """`kernel`: "unified" (plain FP64) or "mixed" (FP32 reduction + FP64
+        refinement). `handles_per_n`: Solver handles per size; a handle whose
+        solver keeps scratch slots serialises its own launches, so two
+        handles let two requests of one N run on the device at once."""
         import torch
         self.torch = torch
         self.dev = torch.device("cuda", device)
         self.slots = slots
         self.pool_size, self.kappa = pool_size, kappa
+        self.kernel = kernel
+        self.handles_per_n = max(1, int(handles_per_n))
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(slots)]
         self._next_stream = 0
-        self.solvers: Dict[int, object] = {}
+        self.solvers: Dict[int, object] = {}          # first handle per N (regime queries)
+        self.handles: Dict[int, list] = {}            # N -> [[solver, requests in flight], ...]
         self.pools: Dict[int, tuple] = {}
         self.poll_sleep_s = poll_sleep_s
 
@@ -229,7 +264,12 @@ class DeviceExecutor:
         for n in sorted(set(sizes)):
             if n in self.solvers:
                 continue
-            self.solvers[n] = Solver(n, device_id=self.dev.index or 0)
+            first = Solver(n, device_id=self.dev.index or 0, kernel=self.kernel)
+            self.solvers[n] = first
+            # smem-cta solvers keep no scratch: one handle serves any overlap
+            count = 1 if first.regime == "smem-cta" else self.handles_per_n
+            self.handles[n] = [[first, 0]] + [[Solver(n, device_id=self.dev.index or 0, kernel=self.kernel), 0]
+                                              for _ in range(count - 1)]
             H, S = baseline_problems_torch(n, self.pool_size, seed=777 + n, kappa=self.kappa, device=self.dev)
             self.pools[n] = (H.transpose(-1, -2).contiguous(), S.transpose(-1, -2).contiguous())
         self.torch.cuda.synchronize(self.dev)
@@ -252,17 +292,29 @@ class DeviceExecutor:
             W = torch.empty((r.q, r.n), dtype=torch.float64, device=self.dev)
             U = torch.empty((r.q, r.n, r.n), dtype=torch.complex128, device=self.dev)
             info = torch.empty((r.q,), dtype=torch.int32, device=self.dev)
-            self.solvers[r.n].launch(H, S, W, U, info, s)
+            slot = min(self.handles[r.n], key=lambda hs: hs[1])    # the least busy handle of this N
+            slot[0].launch(H, S, W, U, info, s)
+            slot[1] += 1
             ev = torch.cuda.Event()
             ev.record(s)
-        return {"event": ev, "out": (W, U, info), "keep": (H, S), "stream": s}
+        return {"event": ev, "out": (W, U, info), "keep": (H, S), "stream": s, "handle": slot}
 
     def finished(self, h):
         return h["event"].query()
 
     def result(self, h):
         h.pop("keep", None)
+        slot = h.pop("handle", None)
+        if slot is not None:
+            slot[1] -= 1
         return h["out"]
+
+    def close(self):
+        for hs in self.handles.values():
+            for solver, _ in hs:
+                solver.close()
+        self.handles.clear()
+        self.solvers.clear()
 
     def wait(self, next_arrival, busy):
         if busy or next_arrival is None:

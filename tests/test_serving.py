@@ -82,3 +82,62 @@ def test_consumer_receives_every_result_once_and_nothing_is_kept():
     assert st.completed == len(reqs) and sorted(rid for rid, _ in got) == sorted(r.rid for r in reqs)
     assert all(res == rid for rid, res in got)          # SimExecutor's result is the request id
     assert all(r.result is None for r in reqs)
+
+
+class _FailingSim(SimExecutor):
+    """SimExecutor whose start() fails with an allocation error for the
+    request ids in `fail_ids`, `times` times each (host-side fault injection:
+    the stand-in for a cudaMalloc / torch allocation that runs out of memory)."""
+
+    def __init__(self, rate, slots, fail_ids, times=1):
+        super().__init__(rate, slots)
+        self.left = {rid: times for rid in fail_ids}
+
+    def start(self, r):
+        if self.left.get(r.rid, 0) > 0:
+            self.left[r.rid] -= 1
+            raise MemoryError(f"injected allocation failure for request {r.rid}")
+        return super().start(r)
+
+
+def test_failed_start_is_retried_after_memory_frees():
+    ex = _FailingSim({8: 100.0}, slots=4, fail_ids=[1])
+    reqs = [Request(rid=0, n=8, q=10, arrival=0.0), Request(rid=1, n=8, q=10, arrival=0.0),
+            Request(rid=2, n=8, q=10, arrival=0.0)]
+    st = ServingEngine(ex, budget_bytes=10 ** 12).run(reqs)
+    assert st.start_failures == 1 and st.failed_requests == 0 and st.completed == 3
+    # request 1 waits for request 0 to finish (0.1 s), then starts; 2 stays behind it (FIFO)
+    assert math.isclose(reqs[0].done, 0.1) and math.isclose(reqs[1].admitted, 0.1)
+    assert math.isclose(reqs[1].done, 0.2) and math.isclose(reqs[2].admitted, 0.1)
+    assert reqs[1].result == 1
+
+
+def test_request_that_never_starts_fails_without_blocking_the_queue():
+    ex = _FailingSim({8: 100.0}, slots=2, fail_ids=[0], times=10 ** 6)
+    reqs = [Request(rid=0, n=8, q=10, arrival=0.0), Request(rid=1, n=8, q=10, arrival=0.05)]
+    st = ServingEngine(ex, budget_bytes=10 ** 12).run(reqs)
+    assert st.failed_requests == 1 and st.completed == 1
+    assert isinstance(reqs[0].result, MemoryError)
+    assert math.isclose(reqs[1].done, 0.15)
+
+
+@pytest.mark.gpu
+def test_mixed_form_serving_matches_plain_within_tolerance(cuda):
+    import torch
+    from sunny_gen_eigensolver_b200.serving import DeviceExecutor
+    sizes = [18, 54]
+    reqs = poisson_requests(400.0, 0.03, sizes, q_range=(16, 64), seed=5)
+    out = {}
+    for kernel in ("unified", "mixed"):
+        ex = DeviceExecutor(slots=4, pool_size=32, kernel=kernel)
+        ex.prepare(sizes)
+        copies = [Request(rid=r.rid, n=r.n, q=r.q, arrival=r.arrival, seed=r.seed) for r in reqs]
+        ServingEngine(ex, budget_bytes=2 * 10 ** 9).run(copies)
+        torch.cuda.synchronize()
+        out[kernel] = {r.rid: r.result for r in copies}
+        ex.close()
+    for rid, (Wp, _, ip) in out["unified"].items():
+        Wm, _, im = out["mixed"][rid]
+        assert torch.equal(ip, im) and bool((ip == 0).all())
+        scale = Wp.abs().amax(dim=1)
+        assert float(((Wm - Wp).abs().amax(dim=1) / scale).max()) <= 1e-12
