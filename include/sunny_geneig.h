@@ -95,10 +95,12 @@ void sunny_geneig_destroy(sunny_geneig_solver_t solver);
  * from several streams: for sizes whose solver keeps scratch slots (the
  * "l2-slot" regime) a launch on a different stream than the previous one
  * waits for it on the device, so launches of one such handle never overlap.
- * A launch captured into a CUDA graph takes part in the same ordering when
- * the graph is replayed (it waits for the handle's latest use enqueued
- * before the replay and marks its own end for later launches); inside one
- * graph, capture each such handle's launches on one stream. */
+ * That ordering covers normal launches only: a launch captured into a CUDA
+ * graph uses the same scratch slots when the graph is replayed, so the
+ * caller must order each replay against other launches and replays of the
+ * same handle (same stream, or an event recorded after one and waited for
+ * before the other); inside one graph, capture each such handle's launches
+ * on one stream. smem-cta handles keep no scratch and need none of this. */
 sunny_geneig_status_t sunny_geneig_launch(
     sunny_geneig_solver_t solver,
     uintptr_t             d_H,

@@ -37,9 +37,6 @@ struct sunny_geneig_solver {
 
 namespace {
 
-// last_stream value after a captured launch: matches no real stream handle
-constexpr uintptr_t kNoStream = ~uintptr_t(0);
-
 thread_local std::string g_last_error;
 
 void set_error(const std::string& msg) { g_last_error = msg; }
@@ -161,28 +158,8 @@ sunny_geneig_status_t launch_impl(sunny_geneig_solver_t s, int stage, uintptr_t 
             e = with_device(s->device, [&]() {
                 const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
                 cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-                if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive) {
-                    // A replay of the graph uses the same scratch slots as the
-                    // handle's normal launches. The captured launch therefore
-                    // waits, at replay time, for the handle's latest recorded use
-                    // (external event-wait node) and records its own end (external
-                    // event-record node), so that replays and normal launches on
-                    // any streams are ordered on the device. Within one graph the
-                    // caller orders this handle's launches (capture them on one
-                    // stream).
-                    if (s->scratch_used) {
-                        cudaError_t w = cudaStreamWaitEvent(st, s->scratch_done, cudaEventWaitExternal);
-                        if (w != cudaSuccess) return w;
-                    }
-                    cudaError_t l = run();
-                    if (l != cudaSuccess) return l;
-                    l = cudaEventRecordWithFlags(s->scratch_done, st, cudaEventRecordExternal);
-                    if (l == cudaSuccess) {
-                        s->scratch_used = true;
-                        s->last_stream = kNoStream;   // the next normal launch always waits
-                    }
-                    return l;
-                }
+                if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+                    return run();   // graph replays are ordered by the caller (see sunny_geneig_launch)
                 if (s->scratch_used && s->last_stream != stream) {
                     cudaError_t w = cudaStreamWaitEvent(st, s->scratch_done, 0);
                     if (w != cudaSuccess) return w;

@@ -721,8 +721,14 @@ static CtaKernelFn cta_kernel_for(int nmax) {
     }
 }
 
+// `smem` is the per-CTA shared-memory limit; the kernel's own static shared
+// memory (profiling builds have some) comes off the dynamic allowance.
 cudaError_t cta_set_attributes(int nmax, size_t smem) {
-    return cudaFuncSetAttribute(cta_kernel_for(nmax), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, cta_kernel_for(nmax));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(cta_kernel_for(nmax), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(smem - fa.sharedSizeBytes));
 }
 
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,

@@ -1050,8 +1050,14 @@ size_t tiled_vec_bytes(int n) {
            (size_t)n * 4 + 8 * 4 + (size_t)dc_vec_ints(n) * 4;
 }
 
+// `smem` is the per-CTA shared-memory limit; the kernel's own static shared
+// memory (profiling builds have some) comes off the dynamic allowance.
 cudaError_t tiled_set_attributes(size_t smem) {
-    return cudaFuncSetAttribute(geneig_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, geneig_tiled_kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(geneig_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(smem - fa.sharedSizeBytes));
 }
 
 cudaError_t tiled_launch(int n, int slots, size_t smem, int stage, const void* H, const void* S, double* W, void* U,

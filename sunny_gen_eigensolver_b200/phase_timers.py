@@ -42,9 +42,11 @@ def main(argv=None) -> dict:
     p.add_argument("--batch", type=int, default=8192)
     p.add_argument("--reps", type=int, default=3)
     p.add_argument("--kappa", type=float, default=100.0)
+    p.add_argument("--lib", type=str, default=None,
+                   help="an already built profiling library to load instead of building lib/'s")
     args = p.parse_args(argv)
 
-    lib = _build.build(phase_timers=True)
+    lib = args.lib or _build.build(phase_timers=True)
     os.environ["SUNNY_GENEIG_LIBPATH"] = str(lib)
     import torch
     from . import _native

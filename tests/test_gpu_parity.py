@@ -297,8 +297,9 @@ def test_create_config_explicit_and_rejected(cuda):
 def test_graph_replay_ordered_with_launches_on_other_streams(cuda):
     """An l2-slot handle (scratch slots shared by all its launches) used both
     by a captured CUDA graph replayed on one stream and by normal launches on
-    another stream: the replays and the launches must not overlap on the
-    device, so every result equals the one-at-a-time result bit for bit."""
+    another stream, with the replays ordered against the launches by the
+    caller as the header asks: every result equals the one-at-a-time result
+    bit for bit, and the capture does not disturb the handle."""
     import torch
     from sunny_gen_eigensolver_b200 import Solver, to_colmajor
     n, batch = 72, 96
@@ -327,8 +328,10 @@ def test_graph_replay_ordered_with_launches_on_other_streams(cuda):
         for _ in range(3):
             with torch.cuda.stream(s1):
                 g.replay()
+            s2.wait_stream(s1)             # the caller orders replays against launches
             s.launch(*bufs[1], stream=s2)
             s.launch(*bufs[1], stream=s2)
+            s1.wait_stream(s2)
         torch.cuda.synchronize()
         for (Hc, Sc, W, U, info), (Wr, Ur, ir) in zip(bufs, ref):
             assert torch.equal(info, ir) and torch.equal(W, Wr) and torch.equal(U, Ur)
