@@ -44,14 +44,23 @@ typedef enum {
 } sunny_geneig_status_t;
 
 /* replaces src/common/c_api.h:32-36. Kernels here are compiled ahead of
- * time, so the cache mode only governs the on-disk launch-shape table. */
+ * time, so the cache holds the autotuner's choices only (see
+ * SUNNY_GENEIG_TUNING_AUTOTUNE): AUTO keeps them in the process and in the
+ * table tune_v1.tsv under $SUNNY_GENEIG_CACHE_DIR (else
+ * $XDG_CACHE_HOME/sunny_geneig, $HOME/.cache/sunny_geneig,
+ * /tmp/sunny_geneig), NODISK in the process only, NOCACHE nowhere. */
 typedef enum {
     SUNNY_GENEIG_CACHE_AUTO    = 0,
     SUNNY_GENEIG_CACHE_NODISK  = 1,
     SUNNY_GENEIG_CACHE_NOCACHE = 2
 } sunny_geneig_cache_mode_t;
 
-/* replaces src/common/c_api.h:38-41 */
+/* replaces src/common/c_api.h:38-41. SUGGESTED: the execution
+ * configuration is chosen by N from measured crossovers. AUTOTUNE: create
+ * times every configuration that can hold N (smem-cta, smem-wide, l2-slot
+ * with 1 or 2 CTAs per SM) on a seeded synthetic batch on the device and
+ * keeps the fastest (cached per N, kernel mode, device and library build
+ * as the cache mode says); the mixed form has a single configuration. */
 typedef enum {
     SUNNY_GENEIG_TUNING_SUGGESTED = 0,
     SUNNY_GENEIG_TUNING_AUTOTUNE  = 1
@@ -68,7 +77,9 @@ typedef enum {
 
 /* replaces src/common/c_api.h:50-55 (impl c_api.cpp:76-107).
  * Returns NULL on failure (message in sunny_geneig_last_error()).
- * batches_per_block_request <= 0 selects automatically. */
+ * batches_per_block_request is accepted for compatibility; every kernel here
+ * solves one matrix pair per CTA at a time (sunny_geneig_batches_per_block
+ * reports 1). */
 sunny_geneig_solver_t sunny_geneig_create(
     int                         n,
     int                         device_id,
@@ -162,6 +173,39 @@ sunny_geneig_status_t sunny_geneig_launch_sigma(
     uintptr_t             d_S,
     uintptr_t             d_W,
     uintptr_t             d_U,
+    uintptr_t             d_info,
+    int                   batch_size,
+    uintptr_t             stream);
+
+/* Spin-wave intensities (no counterpart in the reference's C ABI; the step
+ * Sunny runs after the solve, the reference's benchmarks/sw08_baseline.jl:
+ * 99-103): the metric solve of sunny_geneig_launch_sigma, with each problem's
+ * eigenvectors reduced on the device to its spectrum on an energy grid, so
+ * that U (16 N^2 bytes per problem) never leaves the chip. For the positive
+ * eigenvalues lambda_k, t_k = u_k / sqrt(lambda_k) is the Bogoliubov vector
+ * of the mode of energy omega_k = 1 / lambda_k; with Y = O t_k,
+ *   I_k = sum_ab (delta_ab - qhat_a qhat_b) conj(Y_a) Y_b,
+ *   spec[b * n_energies + e] = sum_k I_k g(energies[e] - omega_k),
+ * g the normalised Gaussian of full width at half maximum fwhm.
+ *   d_O        complex128 3 x N per problem, column-major (element (a, j) of
+ *              problem b at b*3N + 3j + a): the one-body observable matrix
+ *   d_qhat     float64 3 per problem: unit scattering direction
+ *   d_energies float64 n_energies: the energy grid (shared by all problems)
+ *   d_W        float64 N per problem: ascending eigenvalues, as for launch
+ *   d_spec     float64 n_energies per problem
+ * Needs a plain solver in the smem-cta regime (even N <= 64); INVALID_ARG
+ * otherwise, for n_energies < 1 or fwhm <= 0. A failed problem gets its info
+ * code and NaN W and spec. */
+sunny_geneig_status_t sunny_geneig_launch_sigma_intensity(
+    sunny_geneig_solver_t solver,
+    uintptr_t             d_S,
+    uintptr_t             d_O,
+    uintptr_t             d_qhat,
+    uintptr_t             d_energies,
+    int                   n_energies,
+    double                fwhm,
+    uintptr_t             d_W,
+    uintptr_t             d_spec,
     uintptr_t             d_info,
     int                   batch_size,
     uintptr_t             stream);

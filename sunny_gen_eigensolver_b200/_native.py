@@ -29,7 +29,7 @@ EXPORTS = (
     "sunny_geneig_shared_mem_bytes", "sunny_geneig_last_error", "sunny_geneig_path_name",
     "sunny_geneig_kernel_mode", "sunny_geneig_launch_stage", "sunny_geneig_max_matrix_size",
     "sunny_geneig_regime_name", "sunny_geneig_selftest_reciprocal", "sunny_geneig_launch_noalloc",
-    "sunny_geneig_launch_sigma", "sunny_geneig_create_config",
+    "sunny_geneig_launch_sigma", "sunny_geneig_create_config", "sunny_geneig_launch_sigma_intensity",
 )
 
 _lib = None
@@ -66,6 +66,9 @@ def load() -> ctypes.CDLL:
     L.sunny_geneig_launch_stage.restype = c_int
     L.sunny_geneig_launch_sigma.argtypes = [c_void_p, c_size, c_size, c_size, c_size, c_int, c_size]
     L.sunny_geneig_launch_sigma.restype = c_int
+    L.sunny_geneig_launch_sigma_intensity.argtypes = [c_void_p, c_size, c_size, c_size, c_size, c_int,
+                                                      ctypes.c_double, c_size, c_size, c_size, c_int, c_size]
+    L.sunny_geneig_launch_sigma_intensity.restype = c_int
     for name in ("sunny_geneig_matrix_size", "sunny_geneig_batches_per_block", "sunny_geneig_block_dim_x",
                  "sunny_geneig_kernel_mode"):
         getattr(L, name).argtypes = [c_void_p]

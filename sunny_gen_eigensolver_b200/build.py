@@ -21,7 +21,7 @@ LIB_PATH = LIB_DIR / "libsunny_geneig.so"
 TIMERS_LIB_PATH = LIB_DIR / "libsunny_geneig_timers.so"
 INCLUDE = REPO_DIR / "include"
 
-SOURCES = ["geneig_cta.cu", "geneig_plain.cu", "geneig_tiled.cu", "selftest.cu", "c_api.cpp"]
+SOURCES = ["geneig_cta.cu", "geneig_plain.cu", "geneig_tiled.cu", "selftest.cu", "tune.cu", "c_api.cpp"]
 HEADERS = ["geneig_common.cuh", "geneig_dc.cuh", "geneig_kernels.h"]
 
 NVCC_FLAGS = [

@@ -12,10 +12,13 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <exception>
 #include <mutex>
 #include <new>
 #include <string>
+#include <utility>
+#include <vector>
 
 struct sunny_geneig_solver {
     int n = 0;
@@ -24,6 +27,7 @@ struct sunny_geneig_solver {
     sunny_geneig_tuning_mode_t tuning = SUNNY_GENEIG_TUNING_SUGGESTED;
     sunny_geneig_cache_mode_t cache = SUNNY_GENEIG_CACHE_AUTO;
     int bpb = 1;
+    bool tuned = false;          // configuration chosen by the autotuner
     sgeig::PlainPlan plan;
     void* scratch = nullptr;
     // Scratch ordering across streams: a launch that uses the handle's
@@ -102,10 +106,35 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
     s->bpb = 1;
     (void)bpb_request;
     std::string err;
+    std::string tuned_regime;
     e = with_device(device_id, [&]() -> cudaError_t {
+        // TUNING_AUTOTUNE (plain form, no explicit configuration): time every
+        // configuration that can hold n, or take the cached choice
+        if (tuning == SUNNY_GENEIG_TUNING_AUTOTUNE && mode != SUNNY_GENEIG_KERNEL_MIXED &&
+            (regime == nullptr || regime[0] == '\0') && slots_per_sm == 0) {
+            const std::string key = sgeig::tune_key(n, (int)mode, device_id);
+            std::string cfg;
+            if (!sgeig::tune_lookup(key, (int)cache, &cfg)) {
+                const std::vector<std::pair<std::string, int>> cands = {
+                    {"smem-cta", 0}, {"smem-wide", 0}, {"l2-slot", 1}, {"l2-slot", 2}};
+                const int pick = sgeig::tune_pick(n, device_id, cands, &err);
+                if (pick < 0) return cudaErrorInvalidValue;
+                cfg = cands[pick].first + ":" + std::to_string(cands[pick].second);
+                sgeig::tune_store(key, (int)cache, cfg);
+            }
+            const size_t colon = cfg.find(':');
+            tuned_regime = cfg.substr(0, colon);
+            slots_per_sm = colon == std::string::npos ? 0 : std::atoi(cfg.c_str() + colon + 1);
+            regime = tuned_regime.c_str();
+            s->tuned = true;
+        }
         if (!sgeig::plain_plan(n, device_id, &s->plan, &err, mode == SUNNY_GENEIG_KERNEL_MIXED, regime,
-                               slots_per_sm))
-            return cudaErrorInvalidValue;
+                               slots_per_sm)) {
+            // a cached choice this build cannot run any more: the default choice
+            if (!s->tuned || !sgeig::plain_plan(n, device_id, &s->plan, &err, false, nullptr, 0))
+                return cudaErrorInvalidValue;
+            s->tuned = false;
+        }
         if (s->plan.scratch_bytes) {
             cudaError_t ea = cudaMalloc(&s->scratch, s->plan.scratch_bytes);
             if (ea != cudaSuccess) { err = std::string("cudaMalloc scratch: ") + cudaGetErrorString(ea); return ea; }
@@ -268,6 +297,57 @@ sunny_geneig_status_t sunny_geneig_launch_sigma(sunny_geneig_solver_t solver, ui
                                                 uintptr_t d_U, uintptr_t d_info, int batch_size, uintptr_t stream) {
     return launch_impl(solver, 4, 0, d_S, d_W, d_U, d_info, batch_size, stream, "sunny_geneig_launch_sigma",
                        true);
+}
+
+sunny_geneig_status_t sunny_geneig_launch_sigma_intensity(sunny_geneig_solver_t solver, uintptr_t d_S,
+                                                          uintptr_t d_O, uintptr_t d_qhat, uintptr_t d_energies,
+                                                          int n_energies, double fwhm, uintptr_t d_W,
+                                                          uintptr_t d_spec, uintptr_t d_info, int batch_size,
+                                                          uintptr_t stream) {
+    const char* fn = "sunny_geneig_launch_sigma_intensity";
+    clear_error();
+    if (!solver) { set_error(std::string(fn) + ": solver is NULL"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (batch_size < 0) { set_error(std::string(fn) + ": batch_size < 0"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (solver->n & 1) { set_error(std::string(fn) + ": n must be even"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (solver->plan.regime != sgeig::Regime::SmemCta || solver->plan.mixed) {
+        set_error(std::string(fn) + ": needs a plain solver in the smem-cta regime (n <= " +
+                  std::to_string(sgeig::kCtaMaxN) + ")");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (n_energies < 1 || !(fwhm > 0.0)) {
+        set_error(std::string(fn) + ": n_energies must be >= 1 and fwhm > 0");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (batch_size == 0) return SUNNY_GENEIG_OK;
+    if (!d_S || !d_O || !d_qhat || !d_energies || !d_W || !d_spec || !d_info) {
+        set_error(std::string(fn) + ": NULL device buffer");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (!aligned(d_S, 16) || !aligned(d_O, 16) || !aligned(d_qhat, 8) || !aligned(d_energies, 8) ||
+        !aligned(d_W, 8) || !aligned(d_spec, 8) || !aligned(d_info, 4)) {
+        set_error(std::string(fn) + ": misaligned device buffer (S, O need 16 B; qhat, energies, W, spec 8 B)");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    try {
+        const sgeig::PlainPlan& p = solver->plan;
+        cudaError_t e = with_device(solver->device, [&]() {
+            return sgeig::cta_launch_intensity(p.n, p.nmax, p.smem, reinterpret_cast<const void*>(d_S),
+                                               reinterpret_cast<const void*>(d_O),
+                                               reinterpret_cast<const double*>(d_qhat),
+                                               reinterpret_cast<const double*>(d_energies), n_energies, fwhm,
+                                               reinterpret_cast<double*>(d_W), reinterpret_cast<double*>(d_spec),
+                                               reinterpret_cast<int*>(d_info), batch_size,
+                                               reinterpret_cast<cudaStream_t>(stream));
+        });
+        if (e != cudaSuccess) {
+            set_error(std::string(fn) + ": kernel launch failed: " + cudaGetErrorString(e));
+            return SUNNY_GENEIG_LAUNCH_ERROR;
+        }
+    } catch (...) {
+        set_error(std::string("unknown C++ exception in ") + fn);
+        return SUNNY_GENEIG_LAUNCH_ERROR;
+    }
+    return SUNNY_GENEIG_OK;
 }
 
 int sunny_geneig_matrix_size(sunny_geneig_solver_t solver) { return solver ? solver->n : -1; }

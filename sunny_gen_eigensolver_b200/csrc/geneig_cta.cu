@@ -11,24 +11,37 @@
 //       H is read in full, as the reference's two triangular solves do (:246-248)
 //   a5  Householder tridiagonalisation (lower, look-ahead reflector, two
 //       barriers per step), divide and conquer on the tridiagonal,
-//       back-transform V = Q Z in registers per column        (:250)
+//       back-transform V = Q Z in compact-WY blocks of 16 reflectors on the
+//       FP64 tensor cores, one 8-column panel of V per warp          (:250)
 //   a6  U = L^-H V = X^H V on the FP64 tensor cores            (:252)
 //   a7  W (ascending) and U, columns permuted by eigenvalue rank (:268-276)
 //
 // Thread layouts (NT = 256): groups of four lanes (g = tid / 4, q = tid % 4)
-// owning one row or one column for the Cholesky/inverse, the Householder
-// updates and the back-transform; warps owning 8x8 output tiles for the
+// owning one row or one column for the Cholesky/inverse and the Householder
+// updates; warps owning 8x8 output tiles or 8-column panels for the
 // tensor-core GEMMs; a 16 x 16 grid (tr, tc) for the copies.
+//
+// A variant that kept C in registers for the Householder steps (16 x 16
+// thread grid, rank-2 updates in registers) was measured slower on B200 at
+// N = 24 and 54 (80 K vs 75 K and 365 K vs 229 K cycles per solve): the
+// per-warp redundant reflector arithmetic and whole-block predicated
+// updates cost more issue slots than the shared-memory traffic they saved.
 
 #include "geneig_common.cuh"
 #include "geneig_dc.cuh"
 #include "geneig_kernels.h"
+
+#include <cmath>
 
 namespace sgeig {
 namespace {
 
 constexpr int kNT = 256;
 constexpr int kG = 4;
+// stage number of the intensity form (the spin-wave metric solve that
+// reduces U to S(q, E) on the device instead of storing it)
+constexpr int kStageIntensity = 5;
+constexpr int kNG = kNT / kG;
 
 struct CtaArgs {
     const double2* __restrict__ H;
@@ -39,6 +52,14 @@ struct CtaArgs {
     long long batch;
     int n, ld, stage;
     int sigma;      // H = diag(I_{n/2}, -I_{n/2}), not read from memory
+    // stage kStageIntensity (spin-wave intensities in place of U):
+    const double2* O;        // 3 x n observable matrix per problem (column-major)
+    const double*  qhat;     // 3 per problem
+    const double*  energies; // ne
+    double*        spec;     // ne per problem
+    int            ne;
+    double         gnorm;    // Gaussian normalisation 1 / (sigma sqrt(2 pi))
+    double         ginv2;    // 1 / (2 sigma^2)
 };
 
 struct CtaVec {
@@ -157,6 +178,7 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tr = tid >> 4, tc = tid & 15;
     const int g = tid >> 2, q = tid & 3;
+    const unsigned gmask = 0xFu << (lane & ~3);
     const size_t nn = (size_t)n * n;
 
     phase_start();
@@ -325,44 +347,24 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
         }
 
         if (!code) {
-            // ---- a5a: Householder tridiagonalisation of C (lower, the zhetd2 /
-            // zlarfg conventions: reflector k is I - tau_k v v^H on rows k+1..,
-            // v[k+1] = 1, T real). C lives in registers: thread (tr, tc) holds
-            // C(i, j) for i = tr + 16 a, j = tc + 16 b, so a step moves only
-            // vectors through shared memory. Step k:
-            //   P  every warp forms reflector k from column k (colb; C's own
-            //      column 0 in B for k = 0) redundantly, so that no barrier is
-            //      needed; p = tau C22 v from register partial rows reduced
-            //      over the 16 lanes that share them; per-warp partials of p^H v
-            //   -- barrier
-            //   U  w = p + alpha2 v with alpha2 = -tau/2 (p^H v), C22 -= v w^H +
-            //      w v^H in registers; the owners of column k+1 publish it
-            //   -- barrier
-            // Blocks of 16 rows (columns) that lie wholly above (left of) the
-            // active part are skipped. v[k+2..] is also kept in A's strict upper
-            // triangle (row k) for the back-transform, tau_k in v.tau.
-            constexpr int NB = (NMAX + 15) / 16;
-            double2 cr[NB][NB];
-#pragma unroll
-            for (int a_ = 0; a_ < NB; ++a_)
-#pragma unroll
-                for (int b_ = 0; b_ < NB; ++b_) {
-                    const int i = tr + 16 * a_, j = tc + 16 * b_;
-                    cr[a_][b_] = (i < n && j < n) ? B[i + (size_t)j * ld] : c2(0.0, 0.0);
-                }
-            double2* vbuf = v.vb;    // v of the current step (rows > k)
-            double2* colb = v.vb2;   // column k + 1 of the updated matrix (rows > k)
-            for (int k = 0; k < n - 1; ++k) {
-                const double2* col = (k == 0) ? B : colb;
-                const int kb = (k + 1) >> 4;   // first block with an active row
-                // -- P: reflector k (zlarfg), identical in every warp
+            // ---- a5a: Householder tridiagonalisation of C (lower). Reflector k:
+            // I - tau_k v v^H on rows k+1.., v[k+1] = 1, v[k+2..] kept in A's
+            // strict upper triangle (row k), tau_k in v.tau. Look-ahead: during
+            // the rank-2 update of step k, warp 0 updates column k+1 first and
+            // computes reflector k+1 (into the other vector buffer) while warps
+            // 1-7 update the rest, so each step needs two barriers.
+            auto reflect = [&](int k, double2* vbuf) {   // warp 0
+                const double2* bk = B + (size_t)k * ld;
                 double ss = 0.0;
-                for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = col[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
+                for (int i = k + 2 + lane; i < n; i += 32) { const double2 x = bk[i]; ss = fma(x.x, x.x, fma(x.y, x.y, ss)); }
                 ss = warp_sum(ss);
-                const double2 alpha = col[k + 1];
-                double2 taui = c2(0.0, 0.0), scal = c2(0.0, 0.0);
-                double beta = alpha.x;
-                if (!(ss == 0.0 && alpha.y == 0.0)) {
+                const double2 alpha = bk[k + 1];
+                double2 taui, scal = c2(0.0, 0.0);
+                double beta;
+                if (ss == 0.0 && alpha.y == 0.0) {
+                    taui = c2(0.0, 0.0);
+                    beta = alpha.x;
+                } else {
                     beta = -copysign(sqrt(fma(alpha.x, alpha.x, fma(alpha.y, alpha.y, ss))), alpha.x);
                     const double rb = fast_rcp(beta);
                     taui = c2((beta - alpha.x) * rb, -alpha.y * rb);
@@ -370,91 +372,86 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
                     const double inv = fast_rcp(fma(z.x, z.x, z.y * z.y));
                     scal = c2(z.x * inv, -z.y * inv);
                 }
+                for (int i = k + 2 + lane; i < n; i += 32) {
+                    const double2 vi = cmul(bk[i], scal);
+                    vbuf[i] = vi;
+                    A[k + (size_t)i * ld] = vi;
+                }
+                if (lane == 0) {
+                    vbuf[k + 1] = c2(1.0, 0.0);
+                    v.tau[k] = taui;
+                    v.d[k] = bk[k].x;
+                    v.e[k] = beta;
+                }
+            };
+            if (n >= 2 && warp == 0) reflect(0, v.vb);
+            __syncthreads();
+            for (int k = 0; k < n - 1; ++k) {
+                double2* vk = (k & 1) ? v.vb2 : v.vb;
+                double2* vn = (k & 1) ? v.vb : v.vb2;
+                const double2 taui = v.tau[k];
                 const bool has = !(taui.x == 0.0 && taui.y == 0.0);
-                if (warp == (k & 7)) {
-                    for (int i = k + 2 + lane; i < n; i += 32) {
-                        const double2 vi = cmul(col[i], scal);
-                        vbuf[i] = vi;
-                        A[k + (size_t)i * ld] = vi;
-                    }
-                    if (lane == 0) {
-                        vbuf[k + 1] = c2(1.0, 0.0);
-                        v.tau[k] = taui;
-                        v.d[k] = col[k].x;
-                        v.e[k] = beta;
-                    }
-                }
                 if (has) {
-                    double2 vc[NB];
-#pragma unroll
-                    for (int b_ = 0; b_ < NB; ++b_) {
-                        const int j = tc + 16 * b_;
-                        vc[b_] = (j == k + 1) ? c2(1.0, 0.0) : (j > k + 1 && j < n) ? cmul(col[j], scal) : c2(0.0, 0.0);
+                    // p = tau A22 v: four lanes per row; per-warp partial of p^H v
+                    double2 dotp = c2(0.0, 0.0);
+                    for (int i = k + 1 + g; i < n; i += kNG) {
+                        double2 acc = c2(0.0, 0.0);
+                        for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], vk[j]);
+                        acc = group_sum2<kG>(gmask, acc);
+                        const double2 pi = cmul(taui, acc);
+                        if (q == 0) { v.pb[i] = pi; dotp = cfmac(dotp, pi, vk[i]); }
                     }
-                    double2 dp = c2(0.0, 0.0);
-#pragma unroll
-                    for (int a_ = 0; a_ < NB; ++a_) {
-                        if (a_ < kb) continue;
-                        double2 pr = c2(0.0, 0.0);
-#pragma unroll
-                        for (int b_ = 0; b_ < NB; ++b_)
-                            if (b_ >= kb) pr = cfma(pr, cr[a_][b_], vc[b_]);
-                        pr = group_sum2<16>(0xffffffffu, pr);
-                        const int i = tr + 16 * a_;
-                        const double2 pi = (i > k && i < n) ? cmul(taui, pr) : c2(0.0, 0.0);
-                        if (tc == a_ && i < n) v.pb[i] = pi;
-                        if (tc == 0 && i > k && i < n) {
-                            const double2 vi = (i == k + 1) ? c2(1.0, 0.0) : cmul(col[i], scal);
-                            dp = cfmac(dp, pi, vi);
-                        }
-                    }
-                    dp.x += __shfl_xor_sync(0xffffffffu, dp.x, 16);
-                    dp.y += __shfl_xor_sync(0xffffffffu, dp.y, 16);
-                    if (lane == 0) v.wred[warp] = dp;
+                    dotp = warp_sum2(dotp);
+                    if (lane == 0) v.wred[warp] = dotp;
+                    __syncthreads();
                 }
-                __syncthreads();
-                // -- U: rank-2 update in registers
+                // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v)
+                double2 alpha2 = c2(0.0, 0.0);
                 if (has) {
                     double2 dot = c2(0.0, 0.0);
 #pragma unroll
                     for (int w = 0; w < kNT / 32; ++w) dot = cadd(dot, v.wred[w]);
-                    const double2 alpha2 = cscale(cmul(taui, dot), -0.5);
-                    double2 vr[NB], wr[NB];
-#pragma unroll
-                    for (int a_ = 0; a_ < NB; ++a_) {
-                        const int i = tr + 16 * a_;
-                        const bool act = i > k && i < n;
-                        vr[a_] = act ? vbuf[i] : c2(0.0, 0.0);
-                        wr[a_] = act ? cfma(v.pb[i], alpha2, vr[a_]) : c2(0.0, 0.0);
-                    }
-#pragma unroll
-                    for (int b_ = 0; b_ < NB; ++b_) {
-                        if (b_ < kb) continue;
-                        const int j = tc + 16 * b_;
-                        const bool act = j > k && j < n;
-                        const double2 vj = act ? vbuf[j] : c2(0.0, 0.0);
-                        const double2 wj = act ? cfma(v.pb[j], alpha2, vj) : c2(0.0, 0.0);
-#pragma unroll
-                        for (int a_ = 0; a_ < NB; ++a_)
-                            if (a_ >= kb) cr[a_][b_] = cfms_bc(cfms_bc(cr[a_][b_], vr[a_], wj), wr[a_], vj);
-                    }
+                    alpha2 = cscale(cmul(taui, dot), -0.5);
                 }
-                // publish column k + 1 (rows > k) for the next step
-                if (tc == ((k + 1) & 15)) {
-                    const int bsel = (k + 1) >> 4;
-#pragma unroll
-                    for (int a_ = 0; a_ < NB; ++a_) {
-                        const int i = tr + 16 * a_;
-                        double2 x = cr[a_][0];
-#pragma unroll
-                        for (int b_ = 1; b_ < NB; ++b_)
-                            if (b_ == bsel) x = cr[a_][b_];
-                        if (i > k && i < n) colb[i] = x;
+                if (warp == 0) {
+                    if (has) {
+                        const int j = k + 1;
+                        const double2 vj = vk[j];
+                        const double2 wj = cfma(v.pb[j], alpha2, vj);
+                        for (int i = j + lane; i < n; i += 32) {
+                            const double2 vi = vk[i];
+                            const double2 wi = cfma(v.pb[i], alpha2, vi);
+                            double2* p = B + i + (size_t)j * ld;
+                            *p = cfms_bc(cfms_bc(*p, vi, wj), wi, vj);
+                        }
+                        __syncwarp();
+                    }
+                    if (k + 1 < n - 1) reflect(k + 1, vn);
+                } else if (has) {
+                    // group g - 8 of warps 1-7 takes rows k+1+(g-8), +56, ...;
+                    // its lanes take columns j = k+2+q step 4 (column k+1 is warp 0's)
+                    for (int i = k + 1 + (g - 8); i < n; i += kNG - 8) {
+                        const double2 vi = vk[i];
+                        const double2 wi = cfma(v.pb[i], alpha2, vi);
+                        double2* bi = B + i;
+                        int j = k + 2 + q;
+                        for (; j + 4 < n; j += 8) {
+                            const double2 x0 = bi[(size_t)j * ld], x1 = bi[(size_t)(j + 4) * ld];
+                            const double2 v0 = vk[j], v1 = vk[j + 4];
+                            const double2 w0 = cfma(v.pb[j], alpha2, v0), w1 = cfma(v.pb[j + 4], alpha2, v1);
+                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(x0, vi, w0), wi, v0);
+                            bi[(size_t)(j + 4) * ld] = cfms_bc(cfms_bc(x1, vi, w1), wi, v1);
+                        }
+                        if (j < n) {
+                            const double2 v0 = vk[j];
+                            const double2 w0 = cfma(v.pb[j], alpha2, v0);
+                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(bi[(size_t)j * ld], vi, w0), wi, v0);
+                        }
                     }
                 }
                 __syncthreads();
             }
-            if (tid == 0) v.d[n - 1] = (n == 1) ? B[0].x : colb[n - 1].x;
+            if (tid == 0) v.d[n - 1] = B[(n - 1) + (size_t)(n - 1) * ld].x;
             __syncthreads();
             phase_mark(4);
             // ---- a5b: divide and conquer; Z (real) and its workspace in B
@@ -478,7 +475,11 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
 
         if (code) {
             const double qnan = __longlong_as_double(0x7ff8000000000000LL);
-            for (size_t idx = tid; idx < nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
+            if (a.stage == kStageIntensity) {
+                for (int e = tid; e < a.ne; e += kNT) a.spec[(size_t)b * a.ne + e] = qnan;
+            } else {
+                for (size_t idx = tid; idx < nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
+            }
             if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
             if (tid == 0) a.info[b] = code;
             continue;
@@ -693,6 +694,58 @@ __global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(C
             __syncthreads();
             phase_mark(7);
         }
+        if (a.stage == kStageIntensity) {
+            // ---- spin-wave intensities from U (in B, column jj = eigenvalue
+            // dcd[jj]) without storing U: for each positive eigenvalue lambda,
+            // t = u / sqrt(lambda) is the Bogoliubov vector of the mode of
+            // energy omega = 1 / lambda; Y = O t (3 components) and
+            // I = sum_ab (delta_ab - q_a q_b) conj(Y_a) Y_b = |Y|^2 - |q . Y|^2;
+            // then S(E_e) = sum_modes I g(E_e - omega) with the Gaussian g.
+            // A (X) is free after a6 and takes O (3 n <= n ld for even n);
+            // the modes go to the dead Householder vector pb.
+            const double2* Ob = a.O + (size_t)b * 3 * n;
+            double2* Os = A;
+            double* om = reinterpret_cast<double*>(v.pb);
+            double* it = om + n;
+            for (int idx = tid; idx < 3 * n; idx += kNT) Os[idx] = __ldg(Ob + idx);
+            const double q0 = __ldg(a.qhat + 3 * b), q1 = __ldg(a.qhat + 3 * b + 1), q2 = __ldg(a.qhat + 3 * b + 2);
+            __syncthreads();
+            for (int jj = g; jj < n; jj += kNT / kG) {
+                const double lam = v.dcd[jj];
+                double2 y0 = c2(0.0, 0.0), y1 = c2(0.0, 0.0), y2 = c2(0.0, 0.0);
+                for (int i = q; i < n; i += kG) {
+                    const double2 u = B[i + (size_t)jj * ld];
+                    y0 = cfma(y0, Os[3 * i], u);
+                    y1 = cfma(y1, Os[3 * i + 1], u);
+                    y2 = cfma(y2, Os[3 * i + 2], u);
+                }
+                const unsigned gm = 0xFu << (lane & ~3);
+                y0 = group_sum2<kG>(gm, y0);
+                y1 = group_sum2<kG>(gm, y1);
+                y2 = group_sum2<kG>(gm, y2);
+                if (q == 0) {
+                    const double yy = fma(y0.x, y0.x, fma(y0.y, y0.y, fma(y1.x, y1.x, fma(y1.y, y1.y,
+                                      fma(y2.x, y2.x, y2.y * y2.y)))));
+                    const double2 qy = c2(fma(q0, y0.x, fma(q1, y1.x, q2 * y2.x)), fma(q0, y0.y, fma(q1, y1.y, q2 * y2.y)));
+                    const bool pos = lam > 0.0;
+                    om[jj] = pos ? 1.0 / lam : -1.0;
+                    it[jj] = pos ? (yy - fma(qy.x, qy.x, qy.y * qy.y)) / lam : 0.0;
+                }
+            }
+            __syncthreads();
+            for (int e = tid; e < a.ne; e += kNT) {
+                const double E = __ldg(a.energies + e);
+                double acc = 0.0;
+                for (int jj = 0; jj < n; ++jj) {
+                    if (!(om[jj] > 0.0)) continue;
+                    const double x = E - om[jj];
+                    acc = fma(it[jj], exp(-x * x * a.ginv2), acc);
+                }
+                a.spec[(size_t)b * a.ne + e] = acc * a.gnorm;
+            }
+            if (tid == 0) a.info[b] = 0;
+            continue;
+        }
         // ---- a7: store U, column j to position rank[j]
         for (int jj = tr; jj < n; jj += 16) {
             double2* uo = Ub + (size_t)v.rank[jj] * n;
@@ -744,10 +797,43 @@ cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, c
     a.ld = n | 1;
     a.stage = stage;
     a.sigma = sigma ? 1 : 0;
+    a.O = nullptr;
+    a.qhat = a.energies = nullptr;
+    a.spec = nullptr;
+    a.ne = 0;
+    a.gnorm = a.ginv2 = 0.0;
     const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
     cta_kernel_for(nmax)<<<(unsigned)grid, kNT, smem, stream>>>(a);
     return cudaGetLastError();
 }
+
+cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, const void* O, const double* qhat,
+                                 const double* energies, int ne, double fwhm, double* W, double* spec, int* info,
+                                 long long batch, cudaStream_t stream) {
+    CtaArgs a;
+    a.H = nullptr;
+    a.S = static_cast<const double2*>(S);
+    a.W = W;
+    a.U = nullptr;
+    a.info = info;
+    a.batch = batch;
+    a.n = n;
+    a.ld = n | 1;
+    a.stage = kStageIntensity;
+    a.sigma = 1;
+    a.O = static_cast<const double2*>(O);
+    a.qhat = qhat;
+    a.energies = energies;
+    a.spec = spec;
+    a.ne = ne;
+    const double sigma_e = fwhm / (2.0 * std::sqrt(2.0 * std::log(2.0)));
+    a.gnorm = 1.0 / (sigma_e * std::sqrt(2.0 * M_PI));
+    a.ginv2 = 1.0 / (2.0 * sigma_e * sigma_e);
+    const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
+    cta_kernel_for(nmax)<<<(unsigned)grid, kNT, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
 
 }  // namespace sgeig
 

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <string>
+#include <utility>
+#include <vector>
 
 namespace sgeig {
 
@@ -30,6 +32,14 @@ cudaError_t cta_set_attributes(int nmax, size_t smem);
 // `sigma`: H is the metric diag(I_{n/2}, -I_{n/2}) and is not read (H may be NULL).
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
                        int* info, long long batch, cudaStream_t stream, bool sigma = false);
+
+// Spin-wave metric solve that reduces the eigenvectors to the spectrum
+// S(q, E) on the device (no U output): O is 3 x n complex per problem,
+// qhat 3 doubles per problem, energies ne doubles, spec ne doubles per
+// problem; Gaussian broadening of full width at half maximum fwhm.
+cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, const void* O, const double* qhat,
+                                 const double* energies, int ne, double fwhm, double* W, double* spec, int* info,
+                                 long long batch, cudaStream_t stream);
 
 // Tiled kernel for the L2Slot regime (geneig_tiled.cu). A CTA's slot holds,
 // in double2 units, three n x ld complex matrices (four in the mixed form)
@@ -96,5 +106,16 @@ cudaError_t tiled_phase_cycles(unsigned long long* out, int count, bool reset);
 // entry points implemented in other translation units.
 void api_set_error(const std::string& msg);
 void api_clear_error();
+
+// Autotuner behind TUNING_AUTOTUNE (tune.cu). tune_key names a (size, kernel
+// mode, device, library build) pair; tune_lookup / tune_store read and write
+// the cached choice ("regime:slots_per_sm") under `cache_mode` (the C ABI's
+// sunny_geneig_cache_mode_t: 0 memory + disk, 1 memory only, 2 none);
+// tune_pick times the candidate configurations on a synthetic batch on the
+// current device and returns the index of the fastest (-1 if none ran).
+std::string tune_key(int n, int mode, int device);
+bool tune_lookup(const std::string& key, int cache_mode, std::string* config);
+void tune_store(const std::string& key, int cache_mode, const std::string& config);
+int tune_pick(int n, int device, const std::vector<std::pair<std::string, int>>& cands, std::string* err);
 
 }  // namespace sgeig

@@ -149,6 +149,33 @@ class Solver:
         if st != nat.STATUS_OK:
             raise RuntimeError(f"sunny_geneig_launch_sigma failed (status={st}): {nat.last_error()}")
 
+    def launch_sigma_intensity(self, S, O, qhat, energies, fwhm: float, W, spec, info,
+                               stream: Optional[torch.cuda.Stream] = None) -> None:
+        """The metric solve of `launch_sigma` reduced on the device to spin-wave
+        intensities on an energy grid (sunny_geneig_launch_sigma_intensity):
+        S (batch, n, n) column-major buffers, O (batch, n, 3) complex128 (the
+        column-major 3 x n observable matrix per problem), qhat (batch, 3),
+        energies (ne,), W (batch, n), spec (batch, ne) float64, info (batch,).
+        U is never formed in memory."""
+        batch = S.shape[0]
+        n = self.n
+        checks = ((S, (batch, n, n), torch.complex128), (O, (batch, n, 3), torch.complex128),
+                  (qhat, (batch, 3), torch.float64), (W, (batch, n), torch.float64),
+                  (info, (batch,), torch.int32))
+        for t, shape, dt in checks:
+            if tuple(t.shape) != shape or t.dtype != dt or not t.is_cuda or not t.is_contiguous():
+                raise ValueError(f"expected a contiguous CUDA tensor {shape} of {dt}")
+        ne = energies.shape[0]
+        if (energies.dtype != torch.float64 or not energies.is_cuda or not energies.is_contiguous()
+                or tuple(spec.shape) != (batch, ne) or spec.dtype != torch.float64 or not spec.is_contiguous()):
+            raise ValueError("energies (ne,) and spec (batch, ne) must be contiguous float64 CUDA tensors")
+        s = stream if stream is not None else torch.cuda.current_stream(S.device)
+        st = self._lib.sunny_geneig_launch_sigma_intensity(
+            self.handle, S.data_ptr(), O.data_ptr(), qhat.data_ptr(), energies.data_ptr(), int(ne), float(fwhm),
+            W.data_ptr(), spec.data_ptr(), info.data_ptr(), int(batch), s.cuda_stream)
+        if st != nat.STATUS_OK:
+            raise RuntimeError(f"sunny_geneig_launch_sigma_intensity failed (status={st}): {nat.last_error()}")
+
     def run_kernel(self, H: torch.Tensor, S: torch.Tensor, W: Optional[torch.Tensor] = None,
                    U: Optional[torch.Tensor] = None, info: Optional[torch.Tensor] = None,
                    stream: Optional[torch.cuda.Stream] = None) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
