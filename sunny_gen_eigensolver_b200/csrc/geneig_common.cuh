@@ -132,8 +132,9 @@ __device__ __forceinline__ long long& phase_prev() {
     __shared__ long long t;
     return t;
 }
+__device__ __forceinline__ unsigned& phase_level();
 __device__ __forceinline__ void phase_start() {
-    if (threadIdx.x == 0) phase_prev() = clock64();
+    if (threadIdx.x == 0) { phase_prev() = clock64(); phase_level() = 0; }
 }
 __device__ __forceinline__ void phase_mark(int slot) {
     if (threadIdx.x == 0) {
@@ -142,9 +143,27 @@ __device__ __forceinline__ void phase_mark(int slot) {
         phase_prev() = t;
     }
 }
+// Event counters in the same array (profiling builds): phase_count adds v
+// to a slot; phase_level_max keeps the largest v seen since the last
+// phase_level_flush, which (thread 0, after a barrier) adds it to a slot.
+__device__ __forceinline__ unsigned& phase_level() {
+    __shared__ unsigned m;
+    return m;
+}
+__device__ __forceinline__ void phase_count(int slot, unsigned long long v) { atomicAdd(&g_phase_cycles[slot], v); }
+__device__ __forceinline__ void phase_level_max(unsigned v) { atomicMax(&phase_level(), v); }
+__device__ __forceinline__ void phase_level_flush(int slot) {
+    if (threadIdx.x == 0) {
+        atomicAdd(&g_phase_cycles[slot], (unsigned long long)phase_level());
+        phase_level() = 0;
+    }
+}
 #else
 __device__ __forceinline__ void phase_start() {}
 __device__ __forceinline__ void phase_mark(int) {}
+__device__ __forceinline__ void phase_count(int, unsigned long long) {}
+__device__ __forceinline__ void phase_level_max(unsigned) {}
+__device__ __forceinline__ void phase_level_flush(int) {}
 #endif
 
 }  // namespace sgeig

@@ -472,11 +472,17 @@ __device__ void tridiag_dc(int n, DCShared s) {
             const int i = pidx - a, K = s.kcnt[a];
             if (i >= K) continue;
             double t; int o;
-            secular_root_p<4>(i, K, s.dl + a, s.zz + a, s.rho[a], qq, qmask, t, o);
-            if (qq == 0) { s.rt[pidx] = t; s.org[pidx] = o; }
+            const int its = secular_root_p<4>(i, K, s.dl + a, s.zz + a, s.rho[a], qq, qmask, t, o);
+            if (qq == 0) {
+                s.rt[pidx] = t; s.org[pidx] = o;
+                phase_count(27, (unsigned long long)its);
+                phase_count(29, 1);
+                phase_level_max((unsigned)its);
+            }
         }
         __syncthreads();
         phase_mark(12);
+        phase_level_flush(28);
         // ---- phase C: Loewner z-hat, four lanes per root
         for (int p0 = 0; p0 < 4 * n; p0 += NT) {
             const int pidx = (p0 + tid) >> 2, qq = tid & 3;

@@ -34,6 +34,9 @@ PHASES = {
     22: "tiled a5c WY back-transform (+ mixed refinement)", 23: "tiled a6 U = X^H V",
     24: "tiled a7 store U (+ loop barrier)",
 }
+#: event-counter slots (counts, not cycles)
+COUNTERS = {27: "D&C secular iterations", 28: "D&C secular iterations, slowest root per level",
+            29: "D&C secular roots solved"}
 
 
 def main(argv=None) -> dict:
@@ -76,14 +79,18 @@ def main(argv=None) -> dict:
             raise RuntimeError("reading the phase counters failed")
         regime = s.regime
     solves = args.batch * args.reps
-    per = {PHASES.get(k, f"slot {k}"): buf[k] / solves for k in range(32) if buf[k]}
+    per = {PHASES.get(k, f"slot {k}"): buf[k] / solves for k in range(32) if buf[k] and k not in COUNTERS}
+    counts = {name: buf[k] / solves for k, name in COUNTERS.items() if buf[k]}
     total = sum(per.values())
     out = {"n": args.n, "batch": args.batch, "reps": args.reps, "regime": regime,
            "failed": int((info != 0).sum().item()),
            "solves_per_s_timers_build": solves / (ev0.elapsed_time(ev1) * 1e-3),
-           "cycles_per_solve_per_cta": {k: round(v) for k, v in per.items()}, "total_cycles": round(total)}
+           "cycles_per_solve_per_cta": {k: round(v) for k, v in per.items()}, "total_cycles": round(total),
+           "counts_per_solve": {k: round(v, 2) for k, v in counts.items()}}
     for k, v in per.items():
         print(f"{k:42s} {v:10.0f}  {100 * v / total:5.1f} %", file=sys.stderr)
+    for k, v in counts.items():
+        print(f"{k:50s} {v:10.2f} per solve", file=sys.stderr)
     print(json.dumps(out))
     return out
 
