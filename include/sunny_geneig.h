@@ -220,6 +220,37 @@ sunny_geneig_status_t sunny_geneig_launch_sigma_intensity(
 sunny_geneig_solver_t sunny_geneig_create_config(int n, int device_id, sunny_geneig_kernel_mode_t kernel_mode,
                                                  const char* regime, int slots_per_sm);
 
+/* Persistent solver for batches of uneven sizes (no counterpart in the
+ * reference's C ABI). One launch solves problems of up to 8 different sizes,
+ * each size's problems in their own buffers with the layouts, info codes and
+ * NaN fill of sunny_geneig_launch: a device work counter hands out work
+ * items, largest N first, to a grid of 2 CTAs per SM, each item solved by
+ * the same per-problem code as that size's own kernel (results are bitwise
+ * those of per-size launches in the same regime). A work item is one
+ * problem in the l2-slot regime and `per_item` problems in the smem-cta
+ * regime.
+ *   create: sizes[i] distinct, 1 <= sizes[i] <= sunny_geneig_max_matrix_size();
+ *     regimes[i] (NULL = all 0): 0 the default choice by N, 1 smem-cta
+ *     (N <= 64), 2 l2-slot; per_item[i] (NULL or <= 0 = default: 4 in
+ *     smem-cta, 1 in l2-slot). Reserves the l2-slot scratch for the largest
+ *     such size and the work counter. NULL on failure (last_error).
+ *   launch: arrays indexed like `sizes`; counts[i] >= 0 problems of size
+ *     sizes[i] (0 skips the size, its buffers may then be NULL). The launch
+ *     resets the counter on `stream` first (a memset node when captured).
+ *     Launches on different streams are ordered on the device; replays of a
+ *     captured launch must be ordered by the caller, as for sunny_geneig_launch.
+ *   shape: writes the groups in work order (descending N): size, regime (1
+ *     smem-cta, 2 l2-slot) and problems per item; returns their number. */
+typedef struct sunny_geneig_uneven* sunny_geneig_uneven_t;
+sunny_geneig_uneven_t sunny_geneig_uneven_create(int num_sizes, const int* sizes, const int* regimes,
+                                                 const int* per_item, int device_id);
+sunny_geneig_status_t sunny_geneig_uneven_launch(sunny_geneig_uneven_t solver, const uintptr_t* d_H,
+                                                 const uintptr_t* d_S, const uintptr_t* d_W,
+                                                 const uintptr_t* d_U, const uintptr_t* d_info,
+                                                 const int* counts, uintptr_t stream);
+void sunny_geneig_uneven_destroy(sunny_geneig_uneven_t solver);
+int  sunny_geneig_uneven_shape(sunny_geneig_uneven_t solver, int* sizes, int* regimes, int* per_item);
+
 /* Largest N this build accepts in sunny_geneig_create. */
 int sunny_geneig_max_matrix_size(void);
 

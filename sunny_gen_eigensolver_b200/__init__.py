@@ -6,6 +6,6 @@ kernels + C ABI, include/sunny_geneig.h); this package holds its host-side
 binding (`Solver`, mirroring the reference's Julia wrapper), the input
 generators used by the benchmark and the accuracy measures.
 """
-from .solver import Solver, from_colmajor, last_error, solve, to_colmajor  # noqa: F401
+from .solver import Solver, UnevenSolver, from_colmajor, last_error, solve, to_colmajor  # noqa: F401
 
-__all__ = ["Solver", "solve", "to_colmajor", "from_colmajor", "last_error"]
+__all__ = ["Solver", "UnevenSolver", "solve", "to_colmajor", "from_colmajor", "last_error"]

@@ -30,6 +30,8 @@ EXPORTS = (
     "sunny_geneig_kernel_mode", "sunny_geneig_launch_stage", "sunny_geneig_max_matrix_size",
     "sunny_geneig_regime_name", "sunny_geneig_selftest_reciprocal", "sunny_geneig_launch_noalloc",
     "sunny_geneig_launch_sigma", "sunny_geneig_create_config", "sunny_geneig_launch_sigma_intensity",
+    "sunny_geneig_uneven_create", "sunny_geneig_uneven_launch", "sunny_geneig_uneven_destroy",
+    "sunny_geneig_uneven_shape",
 )
 
 _lib = None
@@ -69,6 +71,15 @@ def load() -> ctypes.CDLL:
     L.sunny_geneig_launch_sigma_intensity.argtypes = [c_void_p, c_size, c_size, c_size, c_size, c_int,
                                                       ctypes.c_double, c_size, c_size, c_size, c_int, c_size]
     L.sunny_geneig_launch_sigma_intensity.restype = c_int
+    p_int, p_size = ctypes.POINTER(c_int), ctypes.POINTER(c_size)
+    L.sunny_geneig_uneven_create.argtypes = [c_int, p_int, p_int, p_int, c_int]
+    L.sunny_geneig_uneven_create.restype = c_void_p
+    L.sunny_geneig_uneven_launch.argtypes = [c_void_p, p_size, p_size, p_size, p_size, p_size, p_int, c_size]
+    L.sunny_geneig_uneven_launch.restype = c_int
+    L.sunny_geneig_uneven_destroy.argtypes = [c_void_p]
+    L.sunny_geneig_uneven_destroy.restype = None
+    L.sunny_geneig_uneven_shape.argtypes = [c_void_p, p_int, p_int, p_int]
+    L.sunny_geneig_uneven_shape.restype = c_int
     for name in ("sunny_geneig_matrix_size", "sunny_geneig_batches_per_block", "sunny_geneig_block_dim_x",
                  "sunny_geneig_kernel_mode"):
         getattr(L, name).argtypes = [c_void_p]

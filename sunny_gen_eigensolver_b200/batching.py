@@ -7,6 +7,16 @@ of launches is captured once into a CUDA graph, so that a batch of the same
 shape is re-run by a single graph launch (`UnevenBatch.replay`). The plain
 alternative (`run_sequential`) is one launch per size on one stream.
 
+The persistent form (`persistent` / `replay_persistent`) solves the whole mix
+with ONE kernel launch (sunny_geneig_uneven_*): a device work counter hands
+out items, largest N first, to a grid of 2 CTAs per SM, and each item runs
+the per-problem code of its size's regime (results are bitwise those of
+the per-size launches). `autotune_persistent` picks, per size, the regime
+(smem-cta or l2-slot where both can hold N) and the problems per work item
+(for smem-cta sizes) by timing the one-launch form on the batch's own data,
+one size at a time from the library defaults; the choice is remembered per
+size mix in the same table, and the launch is captured into a CUDA graph.
+
 `autotune` picks, per size class, the execution configuration (which kernel
 regime and, for the l2-slot kernel, how many CTAs per SM: `size_configs`)
 by timing every candidate that can hold that N on the class's own data, and
@@ -26,7 +36,7 @@ from dataclasses import dataclass
 from pathlib import Path
 from typing import Dict, List, Optional, Sequence
 
-TABLE_VERSION = 2
+TABLE_VERSION = 3
 
 
 def size_configs(n: int) -> List[dict]:
@@ -60,14 +70,23 @@ def mix_key(counts: Dict[int, int], device_name: str = "") -> str:
 class Plan:
     streams: List[List[int]]      # sizes launched on each stream, in order
     configs: Dict[int, dict] = None   # size -> {"regime": str, "slots_per_sm": int}
+    # persistent form: size -> {"regime": "smem-cta" | "l2-slot", "per_item": int}
+    persistent: Dict[int, dict] = None
 
     def to_json(self):
-        return {"streams": self.streams, "configs": {str(n): c for n, c in (self.configs or {}).items()}}
+        return {"streams": self.streams, "configs": {str(n): c for n, c in (self.configs or {}).items()},
+                "persistent": {str(n): c for n, c in (self.persistent or {}).items()}}
 
     @staticmethod
     def from_json(d) -> "Plan":
         if not isinstance(d, dict) or not isinstance(d.get("streams"), list):
             raise ValueError("bad plan")
+        pers = {}
+        for k, c in (d.get("persistent") or {}).items():
+            if (not isinstance(c, dict) or c.get("regime") not in ("smem-cta", "l2-slot")
+                    or not isinstance(c.get("per_item"), int) or not 1 <= c["per_item"] <= 64):
+                raise ValueError("bad persistent config")
+            pers[int(k)] = {"regime": c["regime"], "per_item": c["per_item"]}
         st = []
         for lane in d["streams"]:
             if not isinstance(lane, list) or not all(isinstance(x, int) and x > 0 for x in lane):
@@ -81,7 +100,7 @@ class Plan:
                     or c.get("slots_per_sm") not in (0, 1, 2)):
                 raise ValueError("bad size config")
             cfg[int(k)] = {"regime": c["regime"], "slots_per_sm": c["slots_per_sm"]}
-        return Plan(st, cfg)
+        return Plan(st, cfg, pers)
 
 
 class TuneTable:
@@ -172,6 +191,9 @@ class UnevenBatch:
         self.graph = None
         self.plan: Optional[Plan] = None
         self.configs: Dict[int, dict] = {}
+        self.uneven = None               # UnevenSolver of the persistent form
+        self.pgraph = None               # its captured launch
+        self.pconfigs: Dict[int, dict] = {}
 
     @property
     def total(self) -> int:
@@ -305,3 +327,89 @@ class UnevenBatch:
         if table is not None:
             table.put(key, best)
         return best
+
+
+    # ---------------------------------------------------------------- persistent form
+    def persistent(self, configs: Optional[Dict[int, dict]] = None) -> None:
+        """(Re)create the one-launch solver with per-size configurations
+        {n: {"regime": ..., "per_item": ...}} (missing sizes: library defaults)
+        and drop any captured graph of the previous one."""
+        from .solver import UnevenSolver
+        configs = configs or {}
+        if len(self.counts) > 8:
+            raise ValueError("the persistent form takes at most 8 sizes")
+        old = self.uneven
+        self.pgraph = None
+        self.uneven = UnevenSolver(list(self.counts), device_id=self.dev.index or 0,
+                                   regimes={n: c.get("regime") for n, c in configs.items()},
+                                   per_item={n: c.get("per_item") for n, c in configs.items()})
+        if old is not None:
+            self.torch.cuda.synchronize(self.dev)
+            old.close()
+        self.pconfigs = {n: {"regime": r, "per_item": p} for n, r, p in self.uneven.shape}
+
+    def launch_persistent(self, stream=None) -> None:
+        """One launch of the persistent kernel over the whole mix."""
+        if self.uneven is None:
+            self.persistent()
+        self.uneven.launch(self.H, self.S, self.W, self.U, self.info, stream)
+
+    def capture_persistent(self):
+        torch = self.torch
+        if self.uneven is None:
+            self.persistent()
+        s = self._lane_streams(Plan([[0]]))[0]
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        self.launch_persistent(s)                      # warm-up on the capture stream
+        torch.cuda.synchronize(self.dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self.launch_persistent(s)
+        self.pgraph = g
+        return g
+
+    def replay_persistent(self) -> None:
+        if self.pgraph is None:
+            self.capture_persistent()
+        self.pgraph.replay()
+
+    def autotune_persistent(self, table: Optional[TuneTable] = None, per_item_choices=(1, 4, 16)) -> Dict[int, dict]:
+        """Choose each size's regime and problems per item for the one-launch
+        form (see module docstring); remembered per size mix in `table`."""
+        torch = self.torch
+        key = "persistent|" + mix_key(self.counts, torch.cuda.get_device_name(self.dev))
+        if table is not None:
+            known = table.get(key)
+            if known is not None and sorted(known.persistent or {}) == sorted(self.counts):
+                try:
+                    self.persistent(known.persistent)
+                    self.capture_persistent()
+                    return dict(self.pconfigs)
+                except RuntimeError:
+                    pass                                  # a choice this build cannot make: tune again
+        self.persistent()
+        best = dict(self.pconfigs)
+        best_t = self._time(self.launch_persistent, reps=2)
+        for n in sorted(self.counts, key=lambda x: -x):
+            cands = []
+            regimes = ["smem-cta", "l2-slot"] if n <= 64 else ["l2-slot"]
+            for r in regimes:
+                for p in (per_item_choices if r == "smem-cta" else (1,)):
+                    cands.append({"regime": r, "per_item": p})
+            for c in cands:
+                if c == best[n]:
+                    continue
+                trial = dict(best)
+                trial[n] = c
+                try:
+                    self.persistent(trial)
+                except RuntimeError:
+                    continue
+                t = self._time(self.launch_persistent, reps=2)
+                if t < best_t:
+                    best, best_t = dict(self.pconfigs), t
+        self.persistent(best)
+        self.capture_persistent()
+        if table is not None:
+            table.put(key, Plan([sorted(self.counts)], persistent=dict(self.pconfigs)))
+        return dict(self.pconfigs)

@@ -21,8 +21,9 @@ LIB_PATH = LIB_DIR / "libsunny_geneig.so"
 TIMERS_LIB_PATH = LIB_DIR / "libsunny_geneig_timers.so"
 INCLUDE = REPO_DIR / "include"
 
-SOURCES = ["geneig_cta.cu", "geneig_plain.cu", "geneig_tiled.cu", "selftest.cu", "tune.cu", "c_api.cpp"]
-HEADERS = ["geneig_common.cuh", "geneig_dc.cuh", "geneig_kernels.h"]
+SOURCES = ["geneig_cta.cu", "geneig_plain.cu", "geneig_tiled.cu", "geneig_uneven.cu", "selftest.cu", "tune.cu",
+           "c_api.cpp"]
+HEADERS = ["geneig_common.cuh", "geneig_dc.cuh", "geneig_kernels.h", "geneig_cta_body.cuh", "geneig_tiled_body.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

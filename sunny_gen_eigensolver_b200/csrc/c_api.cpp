@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <exception>
@@ -37,6 +38,25 @@ struct sunny_geneig_solver {
     uintptr_t last_stream = 0;
     bool scratch_used = false;
     std::mutex scratch_mu;
+};
+
+// Handle of the persistent uneven-size solver (sunny_geneig_uneven_*).
+struct sunny_geneig_uneven {
+    int device = 0;
+    int ngroups = 0;
+    int order[sgeig::kUnevenMaxGroups] = {};   // caller's index of group g (groups by descending n)
+    int n[sgeig::kUnevenMaxGroups] = {};
+    int kind[sgeig::kUnevenMaxGroups] = {};
+    int per_item[sgeig::kUnevenMaxGroups] = {};
+    size_t smem = 0;
+    int grid = 0;
+    size_t slot_elems = 0;
+    void* scratch = nullptr;
+    unsigned long long* head = nullptr;
+    cudaEvent_t done = nullptr;
+    uintptr_t last_stream = 0;
+    bool used = false;
+    std::mutex mu;
 };
 
 namespace {
@@ -348,6 +368,183 @@ sunny_geneig_status_t sunny_geneig_launch_sigma_intensity(sunny_geneig_solver_t 
         return SUNNY_GENEIG_LAUNCH_ERROR;
     }
     return SUNNY_GENEIG_OK;
+}
+
+sunny_geneig_uneven_t sunny_geneig_uneven_create(int num_sizes, const int* sizes, const int* regimes,
+                                                 const int* per_item, int device_id) {
+    const char* fn = "sunny_geneig_uneven_create";
+    clear_error();
+    try {
+        if (num_sizes < 1 || num_sizes > sgeig::kUnevenMaxGroups || !sizes) {
+            set_error(std::string(fn) + ": num_sizes must be 1.." + std::to_string(sgeig::kUnevenMaxGroups));
+            return nullptr;
+        }
+        for (int i = 0; i < num_sizes; ++i) {
+            if (sizes[i] < 1 || sizes[i] > sgeig::kMaxN) {
+                set_error(std::string(fn) + ": size " + std::to_string(sizes[i]) + " outside [1, " +
+                          std::to_string(sgeig::kMaxN) + "]");
+                return nullptr;
+            }
+            for (int j = 0; j < i; ++j)
+                if (sizes[j] == sizes[i]) {
+                    set_error(std::string(fn) + ": size " + std::to_string(sizes[i]) + " given twice");
+                    return nullptr;
+                }
+            const int r = regimes ? regimes[i] : 0;
+            if (r < 0 || r > 2) {
+                set_error(std::string(fn) + ": regime code must be 0 (default), 1 (smem-cta) or 2 (l2-slot)");
+                return nullptr;
+            }
+            if (r == 1 && sizes[i] > sgeig::kCtaMaxN) {
+                set_error(std::string(fn) + ": smem-cta cannot hold n=" + std::to_string(sizes[i]));
+                return nullptr;
+            }
+        }
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || device_id < 0 || device_id >= count) {
+            set_error(std::string(fn) + ": device_id " + std::to_string(device_id) + " out of range");
+            return nullptr;
+        }
+        auto* h = new sunny_geneig_uneven();
+        h->device = device_id;
+        h->ngroups = num_sizes;
+        for (int i = 0; i < num_sizes; ++i) h->order[i] = i;
+        std::sort(h->order, h->order + num_sizes, [&](int x, int y) { return sizes[x] > sizes[y]; });
+        std::string err;
+        cudaError_t e = with_device(device_id, [&]() -> cudaError_t {
+            int optin = 0, sms = 0;
+            cudaError_t ea = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_id);
+            if (ea == cudaSuccess) ea = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_id);
+            if (ea != cudaSuccess) return ea;
+            size_t slot = 0;
+            for (int g = 0; g < num_sizes; ++g) {
+                const int i = h->order[g], n = sizes[i];
+                const int r = regimes ? regimes[i] : 0;
+                const bool l2 = r == 2 || (r == 0 && n > sgeig::kCtaPreferredMaxN);
+                h->n[g] = n;
+                h->kind[g] = sgeig::uneven_kind(n, l2);
+                h->per_item[g] = (per_item && per_item[i] > 0) ? per_item[i] : (l2 ? 1 : 4);
+                h->smem = std::max(h->smem, sgeig::uneven_smem_bytes(n, h->kind[g]));
+                if (l2) slot = std::max(slot, sgeig::tiled_slot_elems(n));
+            }
+            if (h->smem > (size_t)optin) { err = "the mix needs more shared memory than a CTA has"; return cudaErrorInvalidValue; }
+            ea = sgeig::uneven_set_attributes((size_t)optin);
+            if (ea != cudaSuccess) { err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea); return ea; }
+            h->grid = 2 * sms;
+            h->slot_elems = slot;
+            if (slot) {
+                ea = cudaMalloc(&h->scratch, (size_t)h->grid * slot * 16);
+                if (ea != cudaSuccess) { err = std::string("cudaMalloc scratch: ") + cudaGetErrorString(ea); return ea; }
+            }
+            ea = cudaMalloc(reinterpret_cast<void**>(&h->head), sizeof(unsigned long long));
+            if (ea != cudaSuccess) { err = std::string("cudaMalloc counter: ") + cudaGetErrorString(ea); return ea; }
+            return cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming);
+        });
+        if (e != cudaSuccess) {
+            set_error(std::string(fn) + ": " + (err.empty() ? cudaGetErrorString(e) : err));
+            with_device(device_id, [&]() {
+                cudaFree(h->scratch);
+                cudaFree(h->head);
+                if (h->done) cudaEventDestroy(h->done);
+                return cudaSuccess;
+            });
+            delete h;
+            return nullptr;
+        }
+        return h;
+    } catch (...) {
+        set_error(std::string("unknown C++ exception in ") + fn);
+        return nullptr;
+    }
+}
+
+sunny_geneig_status_t sunny_geneig_uneven_launch(sunny_geneig_uneven_t h, const uintptr_t* d_H,
+                                                 const uintptr_t* d_S, const uintptr_t* d_W,
+                                                 const uintptr_t* d_U, const uintptr_t* d_info,
+                                                 const int* counts, uintptr_t stream) {
+    const char* fn = "sunny_geneig_uneven_launch";
+    clear_error();
+    if (!h) { set_error(std::string(fn) + ": handle is NULL"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (!d_H || !d_S || !d_W || !d_U || !d_info || !counts) {
+        set_error(std::string(fn) + ": NULL array argument");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    sgeig::UnevenLaunch L;
+    L.ngroups = h->ngroups;
+    for (int g = 0; g < h->ngroups; ++g) {
+        const int i = h->order[g];
+        if (counts[i] < 0) { set_error(std::string(fn) + ": negative count"); return SUNNY_GENEIG_INVALID_ARG; }
+        if (counts[i] > 0) {
+            if (!d_H[i] || !d_S[i] || !d_W[i] || !d_U[i] || !d_info[i]) {
+                set_error(std::string(fn) + ": NULL device buffer for size " + std::to_string(h->n[g]));
+                return SUNNY_GENEIG_INVALID_ARG;
+            }
+            if (!aligned(d_H[i], 16) || !aligned(d_S[i], 16) || !aligned(d_U[i], 16) || !aligned(d_W[i], 8) ||
+                !aligned(d_info[i], 4)) {
+                set_error(std::string(fn) + ": misaligned device buffer (H, S, U need 16 B; W 8 B; info 4 B)");
+                return SUNNY_GENEIG_INVALID_ARG;
+            }
+        }
+        L.n[g] = h->n[g];
+        L.kind[g] = h->kind[g];
+        L.per_item[g] = h->per_item[g];
+        L.count[g] = counts[i];
+        L.H[g] = reinterpret_cast<const void*>(d_H[i]);
+        L.S[g] = reinterpret_cast<const void*>(d_S[i]);
+        L.W[g] = reinterpret_cast<double*>(d_W[i]);
+        L.U[g] = reinterpret_cast<void*>(d_U[i]);
+        L.info[g] = reinterpret_cast<int*>(d_info[i]);
+    }
+    try {
+        std::lock_guard<std::mutex> lock(h->mu);
+        cudaError_t e = with_device(h->device, [&]() {
+            const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            const bool capturing = cudaStreamIsCapturing(st, &cs) == cudaSuccess &&
+                                   cs == cudaStreamCaptureStatusActive;
+            if (!capturing && h->used && h->last_stream != stream) {
+                cudaError_t w = cudaStreamWaitEvent(st, h->done, 0);
+                if (w != cudaSuccess) return w;
+            }
+            cudaError_t l = sgeig::uneven_launch(L, h->head, h->scratch, h->slot_elems, h->grid, h->smem, st);
+            if (l != cudaSuccess || capturing) return l;
+            l = cudaEventRecord(h->done, st);
+            if (l == cudaSuccess) { h->used = true; h->last_stream = stream; }
+            return l;
+        });
+        if (e != cudaSuccess) {
+            set_error(std::string(fn) + ": launch failed: " + cudaGetErrorString(e));
+            return SUNNY_GENEIG_LAUNCH_ERROR;
+        }
+    } catch (...) {
+        set_error(std::string("unknown C++ exception in ") + fn);
+        return SUNNY_GENEIG_LAUNCH_ERROR;
+    }
+    return SUNNY_GENEIG_OK;
+}
+
+void sunny_geneig_uneven_destroy(sunny_geneig_uneven_t h) {
+    if (!h) return;
+    try {
+        with_device(h->device, [&]() {
+            if (h->done) { cudaEventSynchronize(h->done); cudaEventDestroy(h->done); }
+            cudaFree(h->scratch);
+            cudaFree(h->head);
+            return cudaSuccess;
+        });
+        delete h;
+    } catch (...) {
+    }
+}
+
+int sunny_geneig_uneven_shape(sunny_geneig_uneven_t h, int* sizes, int* regimes, int* per_item) {
+    if (!h) return -1;
+    for (int g = 0; g < h->ngroups; ++g) {
+        if (sizes) sizes[g] = h->n[g];
+        if (regimes) regimes[g] = h->kind[g] == 5 ? 2 : 1;
+        if (per_item) per_item[g] = h->per_item[g];
+    }
+    return h->ngroups;
 }
 
 int sunny_geneig_matrix_size(sunny_geneig_solver_t solver) { return solver ? solver->n : -1; }

@@ -108,6 +108,23 @@ __host__ __device__ inline int secular_root_p(int i, int K, const double* dl, co
         const double g = 1.0 + lanes_sum<P>(gs, mask);
         if (g >= 0.0) { o = i;     lo = 0.0;  hi = mid; tau = mid; }
         else          { o = i + 1; lo = -mid; hi = 0.0; tau = -mid; }
+        // Starting point: the two nearest poles' terms exactly, the others
+        // frozen at their midpoint value c (the fixed-weight start), i.e. the
+        // root of c + a/(p - x) + b/(q - x) in origin coordinates, taken when
+        // it lies inside the bracket (otherwise the midpoint stays).
+        const double a = rho * zz[i] * zz[i], b = rho * zz[i + 1] * zz[i + 1];
+        const double rm = fast_rcp(mid);
+        const double c = g + (a - b) * rm;
+        const double p0 = dl[i] - dl[o], q0 = dl[i + 1] - dl[o];
+        const double B = -(c * (p0 + q0) + a + b), C = a * q0 + b * p0;
+        if (c != 0.0) {
+            double disc = B * B - 4.0 * c * C;
+            if (disc < 0.0) disc = 0.0;
+            const double qq2 = -0.5 * (B + copysign(sqrt(disc), B));
+            const double x1 = qq2 * fast_rcp(c), x2 = (qq2 != 0.0) ? C * fast_rcp(qq2) : x1;
+            if (x1 > lo && x1 < hi) tau = x1;
+            else if (x2 > lo && x2 < hi) tau = x2;
+        }
     } else {
         double ss = 0.0;
         for (int j = qq; j < K; j += P) ss += zz[j] * zz[j];

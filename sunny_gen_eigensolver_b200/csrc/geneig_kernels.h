@@ -24,8 +24,10 @@ enum class Regime : int {
     L2Slot   = 2,  // any N: working matrices in a per-CTA global-memory slot, tiled MMA kernel
 };
 
-// Shared-memory kernel for N <= 64 (geneig_cta.cu).
+// Shared-memory kernel for N <= 64 (geneig_cta.cu); chosen by default up to
+// kCtaPreferredMaxN (measured crossover with the l2-slot kernel on B200).
 constexpr int kCtaMaxN = 64;
+constexpr int kCtaPreferredMaxN = 60;
 size_t cta_smem_bytes(int n);
 int cta_nmax_for(int n);
 cudaError_t cta_set_attributes(int nmax, size_t smem);
@@ -117,5 +119,30 @@ std::string tune_key(int n, int mode, int device);
 bool tune_lookup(const std::string& key, int cache_mode, std::string* config);
 void tune_store(const std::string& key, int cache_mode, const std::string& config);
 int tune_pick(int n, int device, const std::vector<std::pair<std::string, int>>& cands, std::string* err);
+
+// Persistent uneven-size kernel (geneig_uneven.cu). One launch solves up to
+// kUnevenMaxGroups size groups, given in the order their work is handed out
+// (descending N); kind is uneven_kind(n, l2slot): 0..4 the smem-cta row
+// bound 16/32/48/56/64, 5 the l2-slot body; per_item pencils make one work
+// item. `head` is a device counter (reset by the launch), `scratch` holds
+// `grid` slots of slot_elems complex entries when any group is l2-slot.
+constexpr int kUnevenMaxGroups = 8;
+struct UnevenLaunch {
+    int ngroups = 0;
+    int n[kUnevenMaxGroups] = {};
+    int kind[kUnevenMaxGroups] = {};
+    int per_item[kUnevenMaxGroups] = {};
+    long long count[kUnevenMaxGroups] = {};
+    const void* H[kUnevenMaxGroups] = {};
+    const void* S[kUnevenMaxGroups] = {};
+    double* W[kUnevenMaxGroups] = {};
+    void* U[kUnevenMaxGroups] = {};
+    int* info[kUnevenMaxGroups] = {};
+};
+int uneven_kind(int n, bool l2slot);
+size_t uneven_smem_bytes(int n, int kind);
+cudaError_t uneven_set_attributes(size_t smem);
+cudaError_t uneven_launch(const UnevenLaunch& L, unsigned long long* head, void* scratch, size_t slot_elems,
+                          int grid, size_t smem, cudaStream_t stream);
 
 }  // namespace sgeig

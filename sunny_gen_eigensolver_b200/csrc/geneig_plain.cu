@@ -400,7 +400,6 @@ __global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
 int g_smem_optin = -1;
 
 constexpr int kWideNmax = 96;
-constexpr int kCtaPreferredMaxN = 60;
 
 }  // namespace
 

@@ -16,6 +16,7 @@ as the Julia wrapper raises `error(...)`.
 """
 from __future__ import annotations
 
+import ctypes
 from typing import Optional, Tuple
 
 import torch
@@ -211,6 +212,66 @@ class Solver:
 
 def last_error() -> str:
     return nat.last_error()
+
+
+class UnevenSolver:
+    """Persistent solver for problems of up to 8 different sizes in one launch
+    (sunny_geneig_uneven_*). `regimes[n]` is "smem-cta", "l2-slot" or None
+    (the default choice by n); `per_item[n]` problems of size n make one work
+    item (None: the library default). Buffers are dicts keyed by size, each
+    in the column-major layout of `Solver.launch`."""
+
+    REGIME_CODE = {None: 0, "smem-cta": 1, "l2-slot": 2}
+
+    def __init__(self, sizes, regimes=None, per_item=None, device_id: int = 0):
+        L = nat.load()
+        self.sizes = [int(n) for n in sizes]
+        k = len(self.sizes)
+        regimes = regimes or {}
+        per_item = per_item or {}
+        arr = ctypes.c_int * k
+        h = L.sunny_geneig_uneven_create(k, arr(*self.sizes),
+                                         arr(*[self.REGIME_CODE[regimes.get(n)] for n in self.sizes]),
+                                         arr(*[int(per_item.get(n) or 0) for n in self.sizes]), int(device_id))
+        if not h:
+            raise RuntimeError(f"sunny_geneig_uneven_create failed: {nat.last_error()}")
+        self._lib, self.handle, self.device_id = L, h, int(device_id)
+
+    @property
+    def shape(self):
+        """[(n, regime, problems per item)] in work order (descending n)."""
+        k = len(self.sizes)
+        ns, rs, ps = (ctypes.c_int * k)(), (ctypes.c_int * k)(), (ctypes.c_int * k)()
+        m = self._lib.sunny_geneig_uneven_shape(self.handle, ns, rs, ps)
+        return [(ns[i], "l2-slot" if rs[i] == 2 else "smem-cta", ps[i]) for i in range(m)]
+
+    def launch(self, H, S, W, U, info, stream: Optional[torch.cuda.Stream] = None) -> None:
+        k = len(self.sizes)
+        ptr = lambda d: (ctypes.c_size_t * k)(*[d[n].data_ptr() if n in d else 0 for n in self.sizes])
+        counts = (ctypes.c_int * k)(*[int(H[n].shape[0]) if n in H else 0 for n in self.sizes])
+        dev = next(iter(H.values())).device
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        st = self._lib.sunny_geneig_uneven_launch(self.handle, ptr(H), ptr(S), ptr(W), ptr(U), ptr(info), counts,
+                                                  s.cuda_stream)
+        if st != nat.STATUS_OK:
+            raise RuntimeError(f"sunny_geneig_uneven_launch failed (status={st}): {nat.last_error()}")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.sunny_geneig_uneven_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def solve(H: torch.Tensor, S: torch.Tensor, solver: Optional[Solver] = None,

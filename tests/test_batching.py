@@ -104,3 +104,87 @@ def test_graph_replay_matches_per_size_launches(cuda, tmp_path):
     # the chosen plan and configurations were persisted and are reused
     known = TuneTable(tmp_path / "plans.json").get(mix_key(ub.counts, torch.cuda.get_device_name()))
     assert known is not None and known.configs == plan.configs
+
+
+def test_plan_persistent_configs_roundtrip_and_validation(tmp_path):
+    path = tmp_path / "plans.json"
+    key = "persistent|" + mix_key({12: 100, 216: 10}, "dev")
+    pers = {216: {"regime": "l2-slot", "per_item": 1}, 12: {"regime": "smem-cta", "per_item": 16}}
+    TuneTable(path).put(key, Plan([[12, 216]], persistent=pers))
+    assert TuneTable(path).get(key).persistent == pers
+    raw = json.loads(path.read_text())
+    raw["plans"][key]["persistent"]["12"]["per_item"] = 0
+    path.write_text(json.dumps(raw))
+    assert TuneTable(path).rejected
+
+
+@pytest.mark.gpu
+def test_persistent_launch_matches_per_size_launches(cuda, tmp_path):
+    """The one-launch persistent kernel over a mix of sizes in both regimes
+    (smem-cta 12, 24, 54; l2-slot 72, 108) gives bit for bit what one launch
+    per size gives in the same regime, twice in a row and from a captured
+    graph, with a non-positive-definite problem's info code and NaN fill;
+    the results meet the zhegv bars. autotune_persistent then picks a
+    configuration per size, which is persisted and reused."""
+    import torch
+    from oracle import zhegv_batch
+    from sunny_gen_eigensolver_b200 import Solver, accuracy, generators
+    from sunny_gen_eigensolver_b200.batching import UnevenBatch
+    rng = np.random.default_rng(4)
+    sizes = rng.choice([12, 24, 54, 72, 108], size=400, p=[0.3, 0.2, 0.25, 0.15, 0.1])
+    ub = UnevenBatch(sizes)
+    inputs = {}
+    for n, c in ub.counts.items():
+        H, S = generators.baseline_problems(n, c, seed=100 + n)
+        if n == 24:
+            S[3] = np.eye(n)
+            S[3, 5, 5] = -1.0                       # info = n + 6
+        inputs[n] = (H, S)
+        ub.set_inputs(n, torch.from_numpy(H).cuda().transpose(-1, -2), torch.from_numpy(S).cuda().transpose(-1, -2))
+    ref = {}
+    for n in ub.counts:
+        with Solver(n) as s:
+            s.launch(ub.H[n], ub.S[n], ub.W[n], ub.U[n], ub.info[n])
+            torch.cuda.synchronize()
+        ref[n] = (ub.W[n].clone(), ub.U[n].clone(), ub.info[n].clone())
+    ub.persistent()
+    shape = ub.uneven.shape
+    assert [x[0] for x in shape] == sorted(ub.counts, reverse=True)
+    assert {x[0]: x[1] for x in shape} == {n: ("smem-cta" if n <= 60 else "l2-slot") for n in ub.counts}
+
+    def check():
+        torch.cuda.synchronize()
+        for n in ub.counts:
+            assert torch.equal(ub.info[n], ref[n][2])
+            assert torch.equal(ub.W[n].nan_to_num(7.0), ref[n][0].nan_to_num(7.0))
+            assert torch.equal(ub.U[n].nan_to_num(7.0), ref[n][1].nan_to_num(7.0))
+            ub.W[n].zero_(); ub.U[n].zero_(); ub.info[n].fill_(-1)
+
+    for _ in range(2):
+        ub.launch_persistent()
+        check()
+    ub.capture_persistent()
+    ub.replay_persistent()
+    check()
+    ub.launch_persistent()
+    torch.cuda.synchronize()
+    for n in ub.counts:
+        H, S = inputs[n]
+        info = ub.info[n].cpu().numpy()
+        Wr, _, ir = zhegv_batch(H, S)
+        assert np.array_equal(info, ir)
+        ok = ir == 0
+        W = ub.W[n].cpu().numpy()[ok]
+        U = ub.U[n].transpose(-1, -2).cpu().numpy()[ok]
+        assert accuracy.eig_err_rel(H[ok], W, Wr[ok]).max() <= 1e-12
+        assert accuracy.residual(H[ok], S[ok], W, U).max() <= 1e-12
+    assert ref[24][2][3].item() == 24 + 6
+    table = TuneTable(tmp_path / "plans.json")
+    chosen = ub.autotune_persistent(table)
+    assert sorted(chosen) == sorted(ub.counts)
+    key = "persistent|" + mix_key(ub.counts, torch.cuda.get_device_name())
+    assert TuneTable(tmp_path / "plans.json").get(key).persistent == chosen
+    ub.replay_persistent()
+    torch.cuda.synchronize()
+    for n in ub.counts:
+        assert torch.equal(ub.info[n], ref[n][2])
