@@ -3,6 +3,14 @@
 // (geneig_uneven.cu). The stage chain is described in geneig_cta.cu.
 #pragma once
 
+// How the per-pencil body is compiled into its callers: inlined into the
+// size's own kernel; a caller that dispatches several bodies (the persistent
+// uneven-size kernel) may define it as __noinline__ before including, so
+// that each body keeps its own register allocation.
+#ifndef SGEIG_CTA_BODY_INLINE
+#define SGEIG_CTA_BODY_INLINE __forceinline__
+#endif
+
 #include "geneig_common.cuh"
 #include "geneig_dc.cuh"
 #include "geneig_kernels.h"
@@ -143,7 +151,7 @@ __device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, in
 // One pencil b, solved end to end by the whole CTA (every thread calls
 // this with the same b and the dynamic shared memory of the launch).
 template <int NMAX>
-__device__ __forceinline__ void cta_solve(const CtaArgs& a, long long b, unsigned char* smem_raw) {
+__device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, unsigned char* smem_raw) {
     constexpr int R = NMAX / kG;    // rows per lane in a column group
     const int n = a.n, ld = a.ld;
     const size_t mat = (size_t)n * ld;

@@ -3,6 +3,14 @@
 // The stage chain is described in geneig_tiled.cu.
 #pragma once
 
+// How the per-pencil body is compiled into its callers: inlined into the
+// size's own kernel; a caller that dispatches several bodies (the persistent
+// uneven-size kernel) may define it as __noinline__ before including, so
+// that each body keeps its own register allocation.
+#ifndef SGEIG_TILED_BODY_INLINE
+#define SGEIG_TILED_BODY_INLINE __forceinline__
+#endif
+
 #include "geneig_common.cuh"
 #include "geneig_dc.cuh"
 #include "geneig_kernels.h"
@@ -212,7 +220,7 @@ __device__ __forceinline__ void tri_tile(int t, int& ti, int& tj) {
 // One pencil b, solved end to end by the whole CTA in its global-memory
 // slot `slot` (tiled_slot_elems(n, mixed) complex entries) with the
 // launch's dynamic shared memory as the vector area.
-__device__ __forceinline__ void tiled_solve(const TiledArgs& a, long long b, double2* slot,
+__device__ SGEIG_TILED_BODY_INLINE void tiled_solve(const TiledArgs& a, long long b, double2* slot,
                                             unsigned char* smem_raw) {
     const int n = a.n, ld = a.ld;
     const size_t mat = (size_t)n * ld;
@@ -622,7 +630,6 @@ __device__ __forceinline__ void tiled_solve(const TiledArgs& a, long long b, dou
                         if (c > 0) {
                             for (int i = k + tid; i < n; i += kNT) {
                                 double2 x = ck[i];
-    #pragma unroll 4
                                 for (int cc = 0; cc < c; ++cc) {
                                     x = cfms_bc(x, Vp(i, cc), Wp[k + (size_t)cc * ld]);
                                     x = cfms_bc(x, Wp[i + (size_t)cc * ld], Vp(k, cc));
@@ -667,34 +674,25 @@ __device__ __forceinline__ void tiled_solve(const TiledArgs& a, long long b, dou
                         // (3) y = A v (A: panel-start trailing matrix, read down
                         // column i: y_i = sum_j conj(A(j, i)) v_j), t1 = W^H v and
                         // t2 = V^H v over rows k+1..n; one warp per item
-                        // four items per warp pass, so that each lane has four
-                        // column streams in flight and the reductions overlap
-                        const int m = n - k - 1, items = m + 2 * c;
-                        auto item_at = [&](int it, int j) -> double2 {
-                            if (it < m) return M0[j + (size_t)(k + 1 + it) * ld];
-                            if (it < m + c) return Wp[j + (size_t)(it - m) * ld];
-                            return Vp(j, it - m - c);
-                        };
-                        for (int it0 = warp; it0 < items; it0 += 4 * kNW) {
-                            double2 acc[4] = {zero, zero, zero, zero};
-    #pragma unroll 2
-                            for (int j = k + 1 + lane; j < n; j += 32) {
-                                const double2 vj = v.vb[j];
-    #pragma unroll
-                                for (int u = 0; u < 4; ++u) {
-                                    const int it = it0 + u * kNW;
-                                    if (it < items) acc[u] = cfmac(acc[u], item_at(it, j), vj);
-                                }
+                        const int m = n - k - 1;
+                        for (int it = warp; it < m + 2 * c; it += kNW) {
+                            double2 acc = zero;
+                            if (it < m) {
+                                const int i = k + 1 + it;
+                                const double2* ci = M0 + (size_t)i * ld;
+    #pragma unroll 4
+                                for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, ci[j], v.vb[j]);
+                            } else if (it < m + c) {
+                                const double2* wc = Wp + (size_t)(it - m) * ld;
+                                for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, wc[j], v.vb[j]);
+                            } else {
+                                const int cc = it - m - c;
+                                for (int j = k + 1 + lane; j < n; j += 32) acc = cfmac(acc, Vp(j, cc), v.vb[j]);
                             }
-    #pragma unroll
-                            for (int u = 0; u < 4; ++u) acc[u] = warp_sum2(acc[u]);
+                            acc = warp_sum2(acc);
                             if (lane == 0) {
-    #pragma unroll
-                                for (int u = 0; u < 4; ++u) {
-                                    const int it = it0 + u * kNW;
-                                    if (it < m) v.pb[k + 1 + it] = acc[u];
-                                    else if (it < items) v.red[it - m] = acc[u];   // t1 at red[0..c), t2 at red[c..2c)
-                                }
+                                if (it < m) v.pb[k + 1 + it] = acc;
+                                else v.red[it - m] = acc;      // t1 at red[0..c), t2 at red[c..2c)
                             }
                         }
                         __syncthreads();
@@ -702,7 +700,6 @@ __device__ __forceinline__ void tiled_solve(const TiledArgs& a, long long b, dou
                         // current trailing matrix is A - V W^H - W V^H
                         for (int i = k + 1 + tid; i < n; i += kNT) {
                             double2 x = v.pb[i];
-    #pragma unroll 4
                             for (int cc = 0; cc < c; ++cc) {
                                 x = cfms(x, Vp(i, cc), v.red[cc]);
                                 x = cfms(x, Wp[i + (size_t)cc * ld], v.red[c + cc]);

@@ -11,6 +11,10 @@
 // results are bitwise those of per-size launches. An l2-slot body uses the
 // CTA's own global-memory slot, sized for the largest l2-slot N of the mix.
 
+// The smem-cta bodies are called, each with its own register allocation
+// (inlining all of them with the tiled body into one function made the
+// register allocator spill); the tiled body is inlined into the kernel.
+#define SGEIG_CTA_BODY_INLINE __noinline__
 #include "geneig_cta_body.cuh"
 #include "geneig_tiled_body.cuh"
 
