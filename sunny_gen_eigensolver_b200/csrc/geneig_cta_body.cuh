@@ -206,11 +206,9 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         }
         if (i < n && q == 0) v.colv[i] = x[0];   // column 0, buffer 0
         double ri = 0.0;
-        // a real loop over the columns (slot k of the register row is picked
-        // by predicated moves): fully unrolled, the column loop made the
-        // kernel's code too large for the instruction caches
-#pragma unroll 1
-        for (int k = 0; k < n; ++k) {
+#pragma unroll
+        for (int k = 0; k < NMAX; ++k) {
+            if (k >= n) break;
             __syncthreads();
             const double2* colk = v.colv + (k & 1) * n;
             const double2* rowk = v.rowv + (k & 1) * n;
@@ -234,30 +232,11 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                     if (j > k && j <= i) x[t] = cfms_bc(x[t], aik, colk[j]);
                     else if (j < k) x[t] = cfms(x[t], aik, rowk[j]);
                 }
-                if (q == (k & 3)) {
-                    const double2 nk = cscale(aik, -1.0);
-                    const int kt = k >> 2;
-#pragma unroll
-                    for (int t = 0; t < R; ++t) {
-                        const bool sel = t == kt;
-                        x[t].x = sel ? nk.x : x[t].x;
-                        x[t].y = sel ? nk.y : x[t].y;
-                    }
-                }
+                if (q == (k & 3)) x[k >> 2] = cscale(aik, -1.0);
             }
             // publish column k+1 (rows >= k+1) and row k+1 of acc (j <= k)
             if (k + 1 < n) {
-                if (i >= k + 1 && i < n && q == ((k + 1) & 3)) {
-                    const int kt = (k + 1) >> 2;
-                    double xr = x[0].x, xi = x[0].y;
-#pragma unroll
-                    for (int t = 1; t < R; ++t) {
-                        const bool sel = t == kt;
-                        xr = sel ? x[t].x : xr;
-                        xi = sel ? x[t].y : xi;
-                    }
-                    coln[i] = c2(xr, xi);
-                }
+                if (i >= k + 1 && i < n && q == ((k + 1) & 3)) coln[i] = x[(k + 1) >> 2];
                 if (i == k + 1) {
 #pragma unroll
                     for (int t = 0; t < R; ++t) {
@@ -355,10 +334,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         // strict upper triangle (row k), tau_k in v.tau. Look-ahead: during
         // the rank-2 update of step k, warp 0 updates column k+1 first and
         // computes reflector k+1 (into the other vector buffer) while warps
-        // 1-7 update the rest, so each step needs two barriers. Only the lower
-        // triangle of the trailing matrix is kept up to date (the step is
-        // bound by shared-memory traffic, and this halves the update's); the
-        // matrix-vector product reads A(i, j), j > i, as conj(A(j, i)).
+        // 1-7 update the rest, so each step needs two barriers.
         auto reflect = [&](int k, double2* vbuf) {   // warp 0
             const double2* bk = B + (size_t)k * ld;
             double ss = 0.0;
@@ -402,9 +378,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                 double2 dotp = c2(0.0, 0.0);
                 for (int i = k + 1 + g; i < n; i += kNG) {
                     double2 acc = c2(0.0, 0.0);
-                    int j = k + 1 + q;
-                    for (; j <= i; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], vk[j]);        // row walk
-                    for (; j < n; j += kG) acc = cfma(acc, cconj(B[j + (size_t)i * ld]), vk[j]);   // column walk
+                    for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], vk[j]);
                     acc = group_sum2<kG>(gmask, acc);
                     const double2 pi = cmul(taui, acc);
                     if (q == 0) { v.pb[i] = pi; dotp = cfmac(dotp, pi, vk[i]); }
@@ -436,32 +410,24 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                 }
                 if (k + 1 < n - 1) reflect(k + 1, vn);
             } else if (has) {
-                // the lower triangle of rows k+2.. (column k+1 is warp 0's): group
-                // g - 8 of warps 1-7 takes the row pairs (k+1+t, n-1-t), t = g-8,
-                // +56, ..., whose lengths add up to about the same; its lanes
-                // take columns j = k+2+q step 4 up to the diagonal
-                const int m = n - k - 1;
-                for (int t = g - 8; t < (m + 1) / 2; t += kNG - 8) {
-#pragma unroll
-                    for (int side = 0; side < 2; ++side) {
-                        const int i = side ? n - 1 - t : k + 1 + t;
-                        if (side && i == k + 1 + t) break;     // the middle row of an odd count
-                        const double2 vi = vk[i];
-                        const double2 wi = cfma(v.pb[i], alpha2, vi);
-                        double2* bi = B + i;
-                        int j = k + 2 + q;
-                        for (; j + 4 <= i; j += 8) {
-                            const double2 x0 = bi[(size_t)j * ld], x1 = bi[(size_t)(j + 4) * ld];
-                            const double2 v0 = vk[j], v1 = vk[j + 4];
-                            const double2 w0 = cfma(v.pb[j], alpha2, v0), w1 = cfma(v.pb[j + 4], alpha2, v1);
-                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(x0, vi, w0), wi, v0);
-                            bi[(size_t)(j + 4) * ld] = cfms_bc(cfms_bc(x1, vi, w1), wi, v1);
-                        }
-                        if (j <= i) {
-                            const double2 v0 = vk[j];
-                            const double2 w0 = cfma(v.pb[j], alpha2, v0);
-                            bi[(size_t)j * ld] = cfms_bc(cfms_bc(bi[(size_t)j * ld], vi, w0), wi, v0);
-                        }
+                // group g - 8 of warps 1-7 takes rows k+1+(g-8), +56, ...;
+                // its lanes take columns j = k+2+q step 4 (column k+1 is warp 0's)
+                for (int i = k + 1 + (g - 8); i < n; i += kNG - 8) {
+                    const double2 vi = vk[i];
+                    const double2 wi = cfma(v.pb[i], alpha2, vi);
+                    double2* bi = B + i;
+                    int j = k + 2 + q;
+                    for (; j + 4 < n; j += 8) {
+                        const double2 x0 = bi[(size_t)j * ld], x1 = bi[(size_t)(j + 4) * ld];
+                        const double2 v0 = vk[j], v1 = vk[j + 4];
+                        const double2 w0 = cfma(v.pb[j], alpha2, v0), w1 = cfma(v.pb[j + 4], alpha2, v1);
+                        bi[(size_t)j * ld] = cfms_bc(cfms_bc(x0, vi, w0), wi, v0);
+                        bi[(size_t)(j + 4) * ld] = cfms_bc(cfms_bc(x1, vi, w1), wi, v1);
+                    }
+                    if (j < n) {
+                        const double2 v0 = vk[j];
+                        const double2 w0 = cfma(v.pb[j], alpha2, v0);
+                        bi[(size_t)j * ld] = cfms_bc(cfms_bc(bi[(size_t)j * ld], vi, w0), wi, v0);
                     }
                 }
             }
