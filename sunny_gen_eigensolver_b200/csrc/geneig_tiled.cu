@@ -51,8 +51,8 @@ __global__ void __launch_bounds__(kNT, 2) geneig_tiled_kernel(TiledArgs a) {
 }  // namespace
 
 size_t tiled_vec_bytes(int n) {
-    return (size_t)n * 16 * 3 + 32 * 16 + 3 * 256 * 16 + (size_t)n * 8 * 3 + (size_t)dc_vec_doubles(n) * 8 +
-           (size_t)n * 4 + 8 * 4 + (size_t)dc_vec_ints(n) * 4;
+    return (size_t)n * 16 * 3 + 32 * 16 + 3 * 256 * 16 + tiled_part_elems(n) * 16 + (size_t)n * 8 * 3 +
+           (size_t)dc_vec_doubles(n) * 8 + (size_t)n * 4 + 8 * 4 + (size_t)dc_vec_ints(n) * 4;
 }
 
 // `smem` is the per-CTA shared-memory limit; the kernel's own static shared

@@ -23,6 +23,10 @@ constexpr int kNW = kNT / 32;     // warps per CTA
 // B200 than the 16-column panels (fewer barriers per column); above it the
 // panels' halved trailing-matrix traffic wins (measured crossover ~90).
 constexpr int kBlockedHetrdMinN = 96;
+// Up to this n the blocked reduction forms y = A v column by column with
+// per-warp partial vectors in shared memory (8 n complex entries, which keep
+// two CTAs per SM up to here); above it, a warp per row item.
+constexpr int kColMatvecMaxN = 352;
 
 struct TiledArgs {
     const double2* __restrict__ H;
@@ -93,6 +97,7 @@ struct TVec {
     double2* pb;    // n    tau * A22 * v
     double2* red;   // 32   reduction scratch
     double2* tb;    // 256  T factor of the current WY block (16 x 16, column-major)
+    double2* part;  // tiled_part_elems(n): per-warp partials of the blocked y = A v
     double2* gb;    // 512  Y^H Y of the current WY block: two partial sums, then their sum
     double*  d;     // n    tridiagonal diagonal
     double*  e;     // n    tridiagonal off-diagonal
@@ -103,6 +108,10 @@ struct TVec {
     int*     dci;   // divide-and-conquer ints (dc_vec_ints(n))
 };
 
+__host__ __device__ inline size_t tiled_part_elems(int n) {
+    return (n >= kBlockedHetrdMinN && n <= kColMatvecMaxN) ? (size_t)8 * n : 0;
+}
+
 __device__ inline TVec tcarve(unsigned char* p, int n) {
     TVec v;
     v.tau = reinterpret_cast<double2*>(p);
@@ -111,7 +120,8 @@ __device__ inline TVec tcarve(unsigned char* p, int n) {
     v.red = v.pb + n;
     v.tb  = v.red + 32;
     v.gb  = v.tb + 256;
-    v.d   = reinterpret_cast<double*>(v.gb + 512);
+    v.part = v.gb + 512;
+    v.d   = reinterpret_cast<double*>(v.part + tiled_part_elems(n));
     v.e   = v.d + n;
     v.rdg = v.e + n;
     v.dcd = v.rdg + n;
@@ -671,11 +681,38 @@ __device__ SGEIG_TILED_BODY_INLINE void tiled_solve(const TiledArgs& a, long lon
                         }
                         __syncthreads();
                         const double2 taui = v.tau[k];
-                        // (3) y = A v (A: panel-start trailing matrix, read down
-                        // column i: y_i = sum_j conj(A(j, i)) v_j), t1 = W^H v and
-                        // t2 = V^H v over rows k+1..n; one warp per item
+                        // (3) y = A v (A: panel-start trailing matrix), t1 = W^H v and
+                        // t2 = V^H v over rows k+1..n. Up to kColMatvecMaxN, y is
+                        // formed column by column: warp w takes the contiguous
+                        // columns j = k+1+w, +8, ..., its lanes 4 rows each per
+                        // pass, so every lane keeps a load per row in flight and no
+                        // shuffles are needed; the 8 partials per row are added in
+                        // (4) in a fixed order. Above it, and for t1 / t2, one warp
+                        // per item reads down a column (y_i = sum_j conj(A(j, i)) v_j).
                         const int m = n - k - 1;
-                        for (int it = warp; it < m + 2 * c; it += kNW) {
+                        const bool colmv = n <= kColMatvecMaxN;
+                        if (colmv) {
+                            double2* part = v.part;
+                            for (int r0 = k + 1; r0 < n; r0 += 128) {
+                                double2 acc[4] = {zero, zero, zero, zero};
+    #pragma unroll 2
+                                for (int j = k + 1 + warp; j < n; j += kNW) {
+                                    const double2* cj = M0 + (size_t)j * ld;
+                                    const double2 vj = v.vb[j];
+    #pragma unroll
+                                    for (int u = 0; u < 4; ++u) {
+                                        const int i = r0 + lane + 32 * u;
+                                        if (i < n) acc[u] = cfma(acc[u], cj[i], vj);
+                                    }
+                                }
+    #pragma unroll
+                                for (int u = 0; u < 4; ++u) {
+                                    const int i = r0 + lane + 32 * u;
+                                    if (i < n) part[warp * n + i] = acc[u];
+                                }
+                            }
+                        }
+                        for (int it = (colmv ? m : 0) + warp; it < m + 2 * c; it += kNW) {
                             double2 acc = zero;
                             if (it < m) {
                                 const int i = k + 1 + it;
@@ -700,6 +737,11 @@ __device__ SGEIG_TILED_BODY_INLINE void tiled_solve(const TiledArgs& a, long lon
                         // current trailing matrix is A - V W^H - W V^H
                         for (int i = k + 1 + tid; i < n; i += kNT) {
                             double2 x = v.pb[i];
+                            if (colmv) {
+                                x = zero;
+    #pragma unroll
+                                for (int w = 0; w < kNW; ++w) x = cadd(x, v.part[w * n + i]);
+                            }
                             for (int cc = 0; cc < c; ++cc) {
                                 x = cfms(x, Vp(i, cc), v.red[cc]);
                                 x = cfms(x, Wp[i + (size_t)cc * ld], v.red[c + cc]);
