@@ -303,7 +303,7 @@ __device__ __forceinline__ void dc_merge_tiled(int n, int half, int span, const 
             for (int h = 0; h < 2; ++h)
 #pragma unroll
                 for (int g = 0; g < 2; ++g) acc[h][g][0] = acc[h][g][1] = 0.0;
-#pragma unroll 2
+#pragma unroll 4
             for (int k = 0; k < K; k += 4) {
                 const int ka = k + (lane & 3);
                 const bool kin = ka < K;

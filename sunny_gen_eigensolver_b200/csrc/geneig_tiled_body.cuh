@@ -194,7 +194,7 @@ template <class FA, class FB>
 __device__ __forceinline__ void z16_mma(Z16& c, int i0, int j0, int k0, int k1, FA a_at, FB b_at) {
     const int lane = threadIdx.x & 31;
     const int ar = i0 + (lane >> 2), bc = j0 + (lane >> 2), kq = lane & 3;
-#pragma unroll 2
+#pragma unroll 4
     for (int k = k0; k < k1; k += 4) {
         const int kk = k + kq;
         double2 a[2], b[2];
