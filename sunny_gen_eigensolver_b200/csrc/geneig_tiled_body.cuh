@@ -692,46 +692,24 @@ __device__ SGEIG_TILED_BODY_INLINE void tiled_solve(const TiledArgs& a, long lon
                         const int m = n - k - 1;
                         const bool colmv = n <= kColMatvecMaxN;
                         if (colmv) {
-                            // Only the lower triangle of A is kept (see the trailing
-                            // update), so column j gives y_i += A(i, j) v_j for i >= j
-                            // and y_j += sum_{i > j} conj(A(i, j)) v_i (a warp-reduced
-                            // dot, added by lane 0): each element is read once.
-                            double2* part = v.part + (size_t)warp * n;
-                            for (int i = k + 1 + lane; i < n; i += 32) part[i] = zero;
-                            __syncwarp();
+                            double2* part = v.part;
                             for (int r0 = k + 1; r0 < n; r0 += 128) {
-                                double2 acc[4] = {zero, zero, zero, zero}, vi[4];
-    #pragma unroll
-                                for (int u = 0; u < 4; ++u) {
-                                    const int i = r0 + lane + 32 * u;
-                                    vi[u] = i < n ? v.vb[i] : zero;
-                                }
+                                double2 acc[4] = {zero, zero, zero, zero};
     #pragma unroll 2
                                 for (int j = k + 1 + warp; j < n; j += kNW) {
                                     const double2* cj = M0 + (size_t)j * ld;
                                     const double2 vj = v.vb[j];
-                                    double2 dot = zero;
     #pragma unroll
                                     for (int u = 0; u < 4; ++u) {
                                         const int i = r0 + lane + 32 * u;
-                                        if (i >= j && i < n) {
-                                            const double2 aij = cj[i];
-                                            acc[u] = cfma(acc[u], aij, vj);
-                                            if (i > j) dot = cfmac(dot, aij, vi[u]);
-                                        }
-                                    }
-                                    if (j + 1 < r0 + 128) {       // some row of this chunk lies below j
-                                        dot = warp_sum2(dot);
-                                        if (lane == 0) part[j] = cadd(part[j], dot);
+                                        if (i < n) acc[u] = cfma(acc[u], cj[i], vj);
                                     }
                                 }
-                                __syncwarp();
     #pragma unroll
                                 for (int u = 0; u < 4; ++u) {
                                     const int i = r0 + lane + 32 * u;
-                                    if (i < n) part[i] = cadd(part[i], acc[u]);
+                                    if (i < n) part[warp * n + i] = acc[u];
                                 }
-                                __syncwarp();
                             }
                         }
                         for (int it = (colmv ? m : 0) + warp; it < m + 2 * c; it += kNW) {
@@ -785,19 +763,12 @@ __device__ SGEIG_TILED_BODY_INLINE void tiled_solve(const TiledArgs& a, long lon
                             Wp[i + (size_t)c * ld] = (i > k) ? cfma(v.pb[i], alpha2, v.vb[i]) : zero;
                         __syncthreads();
                     }
-                    // trailing update A(q:n, q:n) -= V W^H + W V^H, q = p + w: lower
-                    // tiles only when the column-oriented product (which reads the
-                    // lower triangle alone) is used, all tiles otherwise
+                    // trailing update A(q:n, q:n) -= V W^H + W V^H, q = p + w (all tiles)
                     const int q = p + w, mq = n - q;
                     if (mq > 0) {
                         const int tq = (mq + 15) >> 4;
-                        const bool lower_only = n <= kColMatvecMaxN;
-                        const int ntiles = lower_only ? tq * (tq + 1) / 2 : tq * tq;
-                        for (int t = warp; t < ntiles; t += kNW) {
-                            int ti, tj;
-                            if (lower_only) tri_tile(t, ti, tj);
-                            else { ti = t / tq; tj = t - ti * tq; }
-                            const int i0 = q + 16 * ti, j0 = q + 16 * tj;
+                        for (int t = warp; t < tq * tq; t += kNW) {
+                            const int ti = t / tq, tj = t - ti * tq, i0 = q + 16 * ti, j0 = q + 16 * tj;
                             Z16 acc;
                             z16_load(acc, i0, j0, [&](int i, int j) { return (i < n && j < n) ? M0[i + (size_t)j * ld] : zero; });
                             z16_mma(acc, i0, j0, 0, w,
