@@ -106,7 +106,9 @@ def run_reference(args):
     if rank != 0:
         return
     from oracle.cpu_baseline import ZhegvPool
-    per_worker = 16
+    # enough problems per worker that a step is ~0.25 s of LAPACK work at N=54,
+    # so that the pool's per-step dispatch is a small part of the time
+    per_worker = max(16, int(256 * (54.0 / args.n) ** 3))
     pool = ZhegvPool(args.n, per_worker=per_worker, kappa=args.kappa)
     solved_per_step = per_worker * pool.workers
     try:
