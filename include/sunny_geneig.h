@@ -15,9 +15,11 @@
  *   d_U      : complex128 N x N x batch; column k of matrix b is the eigenvector
  *              for W[b*N + k], normalised so that U^H S U = I.
  *   d_info   : int32[batch]; 0 on success; N + k when the leading minor of
- *              order k of S is not positive definite (LAPACK zhegv convention);
- *              k in [1, N] when the tridiagonal eigensolver did not converge.
- *              W and U of a failed matrix are filled with NaN.
+ *              order k of S is not positive definite (LAPACK zhegv convention;
+ *              a NaN pivot counts as not positive definite, as in reference
+ *              LAPACK's zpotrf); N - 1 when the tridiagonal eigensolve fails on
+ *              non-finite values (zhegv's count of unconverged off-diagonals;
+ *              0 for N <= 2, as zhegv). W and U of a failed matrix are NaN.
  * Launches are asynchronous on `stream` (0 = legacy default stream); the
  * library never synchronises the host inside a launch.
  * Alignment: d_H, d_S, d_U 16-byte, d_W 8-byte, d_info 4-byte aligned.

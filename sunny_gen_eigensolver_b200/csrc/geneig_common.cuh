@@ -117,6 +117,16 @@ __host__ __device__ __forceinline__ double fast_rcp(double x) {
 // LAPACK dlamch convention: eps = 2^-53 (relative machine precision).
 constexpr double kEps    = 1.1102230246251565e-16;
 
+// ---------------------------------------------------------------- failure codes
+// Internal marker of a failed tridiagonal eigensolve (non-finite values):
+// distinct from every info code (0, 1..n, n+1..2n).
+constexpr int kEigFailCode = -1;
+// The info such a pencil reports, LAPACK zhegv's for the same input: its
+// tridiagonal QR counts the n - 1 off-diagonal elements that did not
+// converge, and for n <= 2 it returns 0 with NaN eigenvalues (W and U are
+// NaN-filled here in every case).
+__host__ __device__ __forceinline__ int eig_fail_info(int n) { return n >= 3 ? n - 1 : 0; }
+
 // ---------------------------------------------------------------- phase timers
 // Profiling builds only (-DSGEIG_PHASE_TIMERS, built as a separate library by
 // build.py --phase-timers): thread 0 of every CTA adds the clock64 cycles

@@ -448,7 +448,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         if (tid == 0) {
             bool bad = false;
             for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
-            v.ctl[4] = bad ? n : 0;
+            v.ctl[4] = bad ? kEigFailCode : 0;
         }
         __syncthreads();
         phase_mark(5);
@@ -463,7 +463,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             for (size_t idx = tid; idx < nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
         }
         if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
-        if (tid == 0) a.info[b] = code;
+        if (tid == 0) a.info[b] = code == kEigFailCode ? eig_fail_info(n) : code;
         return;
     }
 

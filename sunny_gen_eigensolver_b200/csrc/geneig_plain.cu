@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
                 if (tid == 0) {
                     bool bad = false;
                     for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
-                    v.ctl[4] = bad ? n : 0;
+                    v.ctl[4] = bad ? kEigFailCode : 0;
                 }
                 __syncthreads();
                 if (v.ctl[4]) code = v.ctl[4];
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kNT, 1) geneig_plain_kernel(PlainArgs a) {
             const double qnan = __longlong_as_double(0x7ff8000000000000LL);
             for (int idx = tid; idx < (int)nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
             if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
-            if (tid == 0) a.info[b] = code;
+            if (tid == 0) a.info[b] = code == kEigFailCode ? eig_fail_info(n) : code;
             continue;
         }
         if (tid == 0) a.info[b] = 0;

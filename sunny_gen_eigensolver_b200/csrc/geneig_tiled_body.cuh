@@ -806,7 +806,7 @@ __device__ SGEIG_TILED_BODY_INLINE void tiled_solve(const TiledArgs& a, long lon
             if (tid == 0) {
                 bool bad = false;
                 for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
-                v.ctl[4] = bad ? n : 0;
+                v.ctl[4] = bad ? kEigFailCode : 0;
             }
             __syncthreads();
             code = v.ctl[4];
@@ -1071,7 +1071,7 @@ __device__ SGEIG_TILED_BODY_INLINE void tiled_solve(const TiledArgs& a, long lon
         const double qnan = __longlong_as_double(0x7ff8000000000000LL);
         for (int idx = tid; idx < (int)nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
         if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
-        if (tid == 0) a.info[b] = code;
+        if (tid == 0) a.info[b] = code == kEigFailCode ? eig_fail_info(n) : code;
         return;
     }
 

@@ -135,13 +135,19 @@ def test_non_positive_definite_S_info_codes(cuda):
     assert info[3] == 0 and not np.isnan(W[3]).any()
 
 
-def test_nan_input_reports_failure_without_hanging(cuda):
-    H, S = generators.baseline_problems(16, 3, seed=1)
-    H[1, 2, 3] = np.nan
-    H[1, 3, 2] = np.nan
+@pytest.mark.parametrize("n", [2, 16, 54, 72, 108])
+def test_nan_input_info_matches_zhegv(cuda, n):
+    """NaN in H: the info code is zhegv's (n - 1 for n >= 3, 0 for n <= 2:
+    its tridiagonal QR counts every off-diagonal as unconverged) and W and U
+    are NaN; the other problems of the batch are unaffected."""
+    H, S = generators.baseline_problems(n, 3, seed=1)
+    H[1, 0, 1] = np.nan
+    H[1, 1, 0] = np.nan
     W, U, info = gpu_solve(H, S)
-    assert info[0] == 0 and info[2] == 0
-    assert info[1] != 0 or np.isnan(W[1]).any()
+    _, _, ir = zhegv_batch(H, S)
+    assert np.array_equal(info, ir), (info, ir)
+    assert info[1] == (n - 1 if n >= 3 else 0)
+    assert np.isnan(W[1]).all() and np.isnan(U[1]).all()
     check_against_zhegv(H[[0, 2]], S[[0, 2]], W[[0, 2]], U[[0, 2]], info[[0, 2]])
 
 
