@@ -129,6 +129,24 @@ __host__ __device__ inline int secular_root_p(int i, int K, const double* dl, co
         double ss = 0.0;
         for (int j = qq; j < K; j += P) ss += zz[j] * zz[j];
         o = K - 1; lo = 0.0; hi = rho * lanes_sum<P>(ss, mask); tau = hi;
+        // Starting point: the last pole's term exactly, the others frozen at
+        // the bracket's midpoint m (c = f(m) - b / (-m)): the root of
+        // c + b / (-x) = 0, x = b / c, when it lies inside the bracket.
+        const double m = 0.5 * hi;
+        if (m > 0.0) {
+            double gs = 0.0;
+#pragma unroll 4
+            for (int j = qq; j < K; j += P) {
+                const double del = (dl[j] - dl[K - 1]) - m;
+                gs = fma(rho * zz[j], zz[j] * fast_rcp(del), gs);
+            }
+            const double b = rho * zz[K - 1] * zz[K - 1];
+            const double c = 1.0 + lanes_sum<P>(gs, mask) + b * fast_rcp(m);
+            if (c > 0.0) {
+                const double x = b * fast_rcp(c);
+                if (x > lo && x < hi) tau = x;
+            }
+        }
     }
     const double dlo = dl[o];
     const double p = dl[i] - dlo;
