@@ -33,8 +33,14 @@ namespace sgeig {
 using namespace cta;
 namespace {
 
+// CTAs per SM that the register allocation is sized for (65,536 registers
+// shared by that many 256-thread CTAs): small pencils gain more from extra
+// resident CTAs than they lose to the few spills of a tighter budget.
 template <int NMAX>
-__global__ void __launch_bounds__(kNT, (NMAX <= 64) ? 2 : 1) geneig_cta_kernel(CtaArgs a) {
+constexpr int cta_min_blocks() { return NMAX <= 16 ? 4 : NMAX <= 40 ? 3 : 2; }
+
+template <int NMAX>
+__global__ void __launch_bounds__(kNT, cta_min_blocks<NMAX>()) geneig_cta_kernel(CtaArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     phase_start();
     for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) cta_solve<NMAX>(a, b, smem_raw);
@@ -46,13 +52,17 @@ size_t cta_smem_bytes(int n) { return (size_t)2 * n * (n | 1) * 16 + cta_vec_byt
 
 // Compile-time row bounds: the register arrays and unrolled loops are sized by
 // NMAX, so a bound close above n wastes less (56 covers the N=54 workload).
-int cta_nmax_for(int n) { return n <= 16 ? 16 : n <= 32 ? 32 : n <= 48 ? 48 : n <= 56 ? 56 : 64; }
+int cta_nmax_for(int n) {
+    return n <= 16 ? 16 : n <= 24 ? 24 : n <= 32 ? 32 : n <= 40 ? 40 : n <= 48 ? 48 : n <= 56 ? 56 : 64;
+}
 
 using CtaKernelFn = void (*)(CtaArgs);
 static CtaKernelFn cta_kernel_for(int nmax) {
     switch (nmax) {
         case 16: return geneig_cta_kernel<16>;
+        case 24: return geneig_cta_kernel<24>;
         case 32: return geneig_cta_kernel<32>;
+        case 40: return geneig_cta_kernel<40>;
         case 48: return geneig_cta_kernel<48>;
         case 56: return geneig_cta_kernel<56>;
         default: return geneig_cta_kernel<64>;

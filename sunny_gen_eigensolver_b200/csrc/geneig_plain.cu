@@ -563,7 +563,7 @@ cudaError_t noalloc_setup(int dev, NoAllocDevice** out, std::string* err) {
         e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         if (e != cudaSuccess) { *err = std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e); return e; }
         e = tiled_set_attributes((size_t)optin);
-        for (int nmax : {16, 32, 48, 56, 64})
+        for (int nmax : {16, 24, 32, 40, 48, 56, 64})
             if (e == cudaSuccess) e = cta_set_attributes(nmax, (size_t)optin);
         if (e != cudaSuccess) { *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e); return e; }
         d.optin = optin;

@@ -94,8 +94,7 @@ cudaError_t uneven_set_attributes(size_t smem) {
 
 int uneven_kind(int n, bool l2slot) {
     if (l2slot) return 5;
-    const int nmax = cta_nmax_for(n);
-    return nmax == 16 ? 0 : nmax == 32 ? 1 : nmax == 48 ? 2 : nmax == 56 ? 3 : 4;
+    return n <= 16 ? 0 : n <= 32 ? 1 : n <= 48 ? 2 : n <= 56 ? 3 : 4;
 }
 
 size_t uneven_smem_bytes(int n, int kind) {
