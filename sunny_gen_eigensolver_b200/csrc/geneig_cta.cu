@@ -1,6 +1,6 @@
 // Batched generalized Hermitian-definite eigensolver, shared-memory regime
-// (N <= 64): one 256-thread CTA holds one matrix pair in shared memory and
-// solves it end to end; CTAs are persistent over the batch.
+// (N <= 64): one CTA (64 to 256 threads by N) holds one matrix pair in
+// shared memory and solves it end to end; CTAs loop over the batch.
 //
 // Stage chain (reference: src/unified/kernel_source.hpp:233-276):
 //   a1  load S -> A, H -> B                                   (:233-242)
@@ -16,10 +16,10 @@
 //   a6  U = L^-H V = X^H V on the FP64 tensor cores            (:252)
 //   a7  W (ascending) and U, columns permuted by eigenvalue rank (:268-276)
 //
-// Thread layouts (NT = 256): groups of four lanes (g = tid / 4, q = tid % 4)
+// Thread layouts (NT threads): groups of four lanes (g = tid / 4, q = tid % 4)
 // owning one row or one column for the Cholesky/inverse and the Householder
 // updates; warps owning 8x8 output tiles or 8-column panels for the
-// tensor-core GEMMs; a 16 x 16 grid (tr, tc) for the copies.
+// tensor-core GEMMs; an NT/16 x 16 grid (tr, tc) for the copies.
 //
 // A variant that kept C in registers for the Householder steps (16 x 16
 // thread grid, rank-2 updates in registers) was measured slower on B200 at
@@ -33,17 +33,32 @@ namespace sgeig {
 using namespace cta;
 namespace {
 
-// CTAs per SM that the register allocation is sized for (65,536 registers
-// shared by that many 256-thread CTAs): small pencils gain more from extra
-// resident CTAs than they lose to the few spills of a tighter budget.
-template <int NMAX>
-constexpr int cta_min_blocks() { return NMAX <= 16 ? 4 : NMAX <= 40 ? 3 : 2; }
+// Threads per pencil (one pencil per CTA) and CTAs per SM that the register
+// allocation is sized for, by row bound (at least 4 NMAX threads: the
+// Cholesky gives each row a four-lane group). Small pencils run on narrow
+// CTAs, several resident per SM: their steps are latency chains (a barrier
+// per Cholesky column, two per Householder step), so more pencils in flight
+// raise throughput more than more threads per pencil. Measured on B200
+// (solves/s at batch 65,536, against 256 threads and 2-3 CTAs/SM):
+//   NMAX 16: 64 x 8   N=16 9.09 M (3.80 M); 64 x 16 (spills) 7.36 M
+//   NMAX 24: 128 x 4  N=24 4.45 M (2.42 M); 96 x 4 4.39 M, 128 x 6 2.85 M
+//   NMAX 32: 128 x 4  N=32 2.26 M (1.96 M); 128 x 5 2.09 M
+//   NMAX 40: 256 x 3  N=40 1.36 M; 160 x 3 1.31 M, 192 x 3 1.34 M
+//   NMAX 48: 192 x 2  N=44 1.16 M (1.08 M); N=48 0.97 M either way
+//   NMAX 56: 256 x 2  N=54 832 K; 224 x 2 748 K
+template <int NMAX> struct CtaShape { static constexpr int nt = kNT, minb = 2; };
+template <> struct CtaShape<16> { static constexpr int nt = 64, minb = 8; };
+template <> struct CtaShape<24> { static constexpr int nt = 128, minb = 4; };
+template <> struct CtaShape<32> { static constexpr int nt = 128, minb = 4; };
+template <> struct CtaShape<40> { static constexpr int nt = kNT, minb = 3; };
+template <> struct CtaShape<48> { static constexpr int nt = 192, minb = 2; };
 
 template <int NMAX>
-__global__ void __launch_bounds__(kNT, cta_min_blocks<NMAX>()) geneig_cta_kernel(CtaArgs a) {
+__global__ void __launch_bounds__(CtaShape<NMAX>::nt, CtaShape<NMAX>::minb) geneig_cta_kernel(CtaArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     phase_start();
-    for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) cta_solve<NMAX>(a, b, smem_raw);
+    for (long long b = blockIdx.x; b < a.batch; b += gridDim.x)
+        cta_solve<NMAX, CtaShape<NMAX>::nt>(a, b, smem_raw);
 }
 
 }  // namespace
@@ -66,6 +81,18 @@ static CtaKernelFn cta_kernel_for(int nmax) {
         case 48: return geneig_cta_kernel<48>;
         case 56: return geneig_cta_kernel<56>;
         default: return geneig_cta_kernel<64>;
+    }
+}
+
+int cta_threads_for(int nmax) {
+    switch (nmax) {
+        case 16: return CtaShape<16>::nt;
+        case 24: return CtaShape<24>::nt;
+        case 32: return CtaShape<32>::nt;
+        case 40: return CtaShape<40>::nt;
+        case 48: return CtaShape<48>::nt;
+        case 56: return CtaShape<56>::nt;
+        default: return CtaShape<64>::nt;
     }
 }
 
@@ -98,7 +125,7 @@ cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, c
     a.ne = 0;
     a.gnorm = a.ginv2 = 0.0;
     const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
-    cta_kernel_for(nmax)<<<(unsigned)grid, kNT, smem, stream>>>(a);
+    cta_kernel_for(nmax)<<<(unsigned)grid, cta_threads_for(nmax), smem, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -125,7 +152,7 @@ cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, co
     a.gnorm = 1.0 / (sigma_e * std::sqrt(2.0 * M_PI));
     a.ginv2 = 1.0 / (2.0 * sigma_e * sigma_e);
     const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
-    cta_kernel_for(nmax)<<<(unsigned)grid, kNT, smem, stream>>>(a);
+    cta_kernel_for(nmax)<<<(unsigned)grid, cta_threads_for(nmax), smem, stream>>>(a);
     return cudaGetLastError();
 }
 

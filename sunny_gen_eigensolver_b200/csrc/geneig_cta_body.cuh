@@ -24,7 +24,6 @@ constexpr int kG = 4;
 // stage number of the intensity form (the spin-wave metric solve that
 // reduces U to S(q, E) on the device instead of storing it)
 constexpr int kStageIntensity = 5;
-constexpr int kNG = kNT / kG;
 
 struct CtaArgs {
     const double2* __restrict__ H;
@@ -106,10 +105,10 @@ struct ZTiles {
     double re[MAXT][2], im[MAXT][2];
 };
 
-template <int MAXT, class FA, class FB, class FK, class FKeep>
+template <int MAXT, int NT, class FA, class FB, class FK, class FKeep>
 __device__ __forceinline__ void ztiles_compute(ZTiles<MAXT>& acc, int tm, int tn, FA fa, FB fb, FK kr, FKeep keep) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = kNT / 32;
+    constexpr int NW = NT / 32;
 #pragma unroll
     for (int u = 0; u < MAXT; ++u) {
         acc.re[u][0] = acc.re[u][1] = acc.im[u][0] = acc.im[u][1] = 0.0;
@@ -132,10 +131,10 @@ __device__ __forceinline__ void ztiles_compute(ZTiles<MAXT>& acc, int tm, int tn
     }
 }
 
-template <int MAXT, class FKeep, class FPut>
+template <int MAXT, int NT, class FKeep, class FPut>
 __device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, int tn, FKeep keep, FPut put) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = kNT / 32;
+    constexpr int NW = NT / 32;
 #pragma unroll
     for (int u = 0; u < MAXT; ++u) {
         const int t = warp + NW * u;
@@ -148,11 +147,17 @@ __device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, in
     }
 }
 
-// One pencil b, solved end to end by the whole CTA (every thread calls
-// this with the same b and the dynamic shared memory of the launch).
-template <int NMAX>
+// One pencil b, solved end to end by the whole CTA of NT threads (every
+// thread calls this with the same b and the dynamic shared memory of the
+// launch). NT >= 4 NMAX: the Cholesky gives each row a column group of
+// four lanes.
+template <int NMAX, int NT = kNT>
 __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, unsigned char* smem_raw) {
     constexpr int R = NMAX / kG;    // rows per lane in a column group
+    constexpr int NW = NT / 32;     // warps
+    constexpr int NG = NT / kG;     // column groups
+    constexpr int TR = NT / 16;     // thread rows of the 16-wide copy loops
+    static_assert(NG >= NMAX && NW >= 2 && NW <= 8 && NT % 32 == 0, "CTA shape");
     const int n = a.n, ld = a.ld;
     const size_t mat = (size_t)n * ld;
     double2* A = reinterpret_cast<double2*>(smem_raw);
@@ -173,7 +178,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     __syncthreads();
     phase_mark(8);
     // ---- a1: load (rows by tc so that global reads are contiguous)
-    for (int j = tr; j < n; j += 16)
+    for (int j = tr; j < n; j += TR)
         for (int i = tc; i < n; i += 16) {
             A[i + (size_t)j * ld] = __ldg(Sb + i + (size_t)j * n);
             if (!a.sigma) B[i + (size_t)j * ld] = __ldg(Hb + i + (size_t)j * n);
@@ -221,7 +226,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             if (i == k) ri = r;
             if (tid == 0) v.rdg[k] = r;
             if (a.stage == 1) {   // stage-wise output: column k of L
-                for (int jj = k + tid; jj < n; jj += kNT)
+                for (int jj = k + tid; jj < n; jj += NT)
                     A[jj + (size_t)k * ld] = (jj == k) ? c2(1.0 / r, 0.0) : cscale(colk[jj], r);
             }
             if (i > k && i < n) {
@@ -262,7 +267,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     int code = fail ? n + fail : 0;   // zhegv: info = n + order of the failing minor
 
     if (!code && a.stage == 1) {
-        for (int j = tr; j < n; j += 16)
+        for (int j = tr; j < n; j += TR)
             for (int i = tc; i < n; i += 16)
                 Ub[i + (size_t)j * n] = (i >= j) ? A[i + (size_t)j * ld] : c2(0.0, 0.0);
         if (tid == 0) a.info[b] = 0;
@@ -273,12 +278,12 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         // A now holds X = L^-1 in its lower triangle (diagonal real).
         // ---- a3: T = H X^H, T(i, j) = sum_{k <= j} H(i, k) conj(X(j, k)),
         // FP64 tensor-core tiles; T overwrites H after the barrier.
-        constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + kNT / 32 - 1) / (kNT / 32);
+        constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + NW - 1) / NW;
         const int tn8 = (n + 7) >> 3;
         if (a.sigma) {
             // H = diag(I, -I): T(i, j) = sigma_i conj(X(j, i)), no product needed
             const int m = n >> 1;
-            for (int j = tr; j < n; j += 16)
+            for (int j = tr; j < n; j += TR)
                 for (int i = tc; i < n; i += 16) {
                     const double2 x = (i <= j) ? cconj(A[j + (size_t)i * ld]) : c2(0.0, 0.0);
                     B[i + (size_t)j * ld] = (i < m) ? x : c2(-x.x, -x.y);
@@ -286,13 +291,13 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             __syncthreads();
         } else {
             ZTiles<MAXT> acc;
-            ztiles_compute<MAXT>(acc, tn8, tn8,
+            ztiles_compute<MAXT, NT>(acc, tn8, tn8,
                 [&](int i, int k) { return (i < n && k < n) ? B[i + (size_t)k * ld] : c2(0.0, 0.0); },
                 [&](int k, int j) { return (j < n && k <= j) ? cconj(A[j + (size_t)k * ld]) : c2(0.0, 0.0); },
                 [&](int, int tj, int& k0, int& k1) { k0 = 0; k1 = min(n, 8 * tj + 8); },
                 [](int, int) { return true; });
             __syncthreads();
-            ztiles_store<MAXT>(acc, tn8, tn8, [](int, int) { return true; },
+            ztiles_store<MAXT, NT>(acc, tn8, tn8, [](int, int) { return true; },
                 [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
             __syncthreads();
         }
@@ -302,13 +307,13 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         // C is exactly Hermitian.
         {
             ZTiles<MAXT> acc;
-            ztiles_compute<MAXT>(acc, tn8, tn8,
+            ztiles_compute<MAXT, NT>(acc, tn8, tn8,
                 [&](int i, int k) { return (i < n && k <= i) ? A[i + (size_t)k * ld] : c2(0.0, 0.0); },
                 [&](int k, int j) { return (k < n && j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0); },
                 [&](int ti, int, int& k0, int& k1) { k0 = 0; k1 = min(n, 8 * ti + 8); },
                 [](int ti, int tj) { return ti >= tj; });
             __syncthreads();
-            ztiles_store<MAXT>(acc, tn8, tn8, [](int ti, int tj) { return ti >= tj; },
+            ztiles_store<MAXT, NT>(acc, tn8, tn8, [](int ti, int tj) { return ti >= tj; },
                 [&](int i, int j, double2 c) {
                     if (i < n && j < n && i >= j) {
                         if (i == j) c.y = 0.0;
@@ -322,7 +327,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     }
 
     if (!code && a.stage == 2) {
-        for (int j = tr; j < n; j += 16)
+        for (int j = tr; j < n; j += TR)
             for (int i = tc; i < n; i += 16) Ub[i + (size_t)j * n] = B[i + (size_t)j * ld];
         if (tid == 0) a.info[b] = 0;
         return;
@@ -333,8 +338,8 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         // I - tau_k v v^H on rows k+1.., v[k+1] = 1, v[k+2..] kept in A's
         // strict upper triangle (row k), tau_k in v.tau. Look-ahead: during
         // the rank-2 update of step k, warp 0 updates column k+1 first and
-        // computes reflector k+1 (into the other vector buffer) while warps
-        // 1-7 update the rest, so each step needs two barriers.
+        // computes reflector k+1 (into the other vector buffer) while the
+        // other warps update the rest, so each step needs two barriers.
         auto reflect = [&](int k, double2* vbuf) {   // warp 0
             const double2* bk = B + (size_t)k * ld;
             double ss = 0.0;
@@ -376,7 +381,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             if (has) {
                 // p = tau A22 v: four lanes per row; per-warp partial of p^H v
                 double2 dotp = c2(0.0, 0.0);
-                for (int i = k + 1 + g; i < n; i += kNG) {
+                for (int i = k + 1 + g; i < n; i += NG) {
                     double2 acc = c2(0.0, 0.0);
                     for (int j = k + 1 + q; j < n; j += kG) acc = cfma(acc, B[i + (size_t)j * ld], vk[j]);
                     acc = group_sum2<kG>(gmask, acc);
@@ -392,7 +397,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             if (has) {
                 double2 dot = c2(0.0, 0.0);
 #pragma unroll
-                for (int w = 0; w < kNT / 32; ++w) dot = cadd(dot, v.wred[w]);
+                for (int w = 0; w < NW; ++w) dot = cadd(dot, v.wred[w]);
                 alpha2 = cscale(cmul(taui, dot), -0.5);
             }
             if (warp == 0) {
@@ -410,9 +415,9 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                 }
                 if (k + 1 < n - 1) reflect(k + 1, vn);
             } else if (has) {
-                // group g - 8 of warps 1-7 takes rows k+1+(g-8), +56, ...;
+                // group g - 8 of warps 1.. takes rows k+1+(g-8), + NG-8, ...;
                 // its lanes take columns j = k+2+q step 4 (column k+1 is warp 0's)
-                for (int i = k + 1 + (g - 8); i < n; i += kNG - 8) {
+                for (int i = k + 1 + (g - 8); i < n; i += NG - 8) {
                     const double2 vi = vk[i];
                     const double2 wi = cfma(v.pb[i], alpha2, vi);
                     double2* bi = B + i;
@@ -444,7 +449,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         dc.w = v.dcd; dc.z = dc.w + n; dc.dl = dc.z + n; dc.zz = dc.dl + n; dc.zh = dc.zz + n;
         dc.rt = dc.zh + n; dc.rho = dc.rt + n; dc.scal = dc.rho + n;
         dc.org = v.dci; dc.nd = dc.org + n; dc.perm = dc.nd + n; dc.kcnt = dc.perm + n;
-        tridiag_dc<kNT, NMAX>(n, dc);
+        tridiag_dc<NT, NMAX>(n, dc);
         if (tid == 0) {
             bool bad = false;
             for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
@@ -458,17 +463,17 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     if (code) {
         const double qnan = __longlong_as_double(0x7ff8000000000000LL);
         if (a.stage == kStageIntensity) {
-            for (int e = tid; e < a.ne; e += kNT) a.spec[(size_t)b * a.ne + e] = qnan;
+            for (int e = tid; e < a.ne; e += NT) a.spec[(size_t)b * a.ne + e] = qnan;
         } else {
-            for (size_t idx = tid; idx < nn; idx += kNT) Ub[idx] = c2(qnan, qnan);
+            for (size_t idx = tid; idx < nn; idx += NT) Ub[idx] = c2(qnan, qnan);
         }
-        if (a.stage >= 3) for (int i = tid; i < n; i += kNT) Wb[i] = qnan;
+        if (a.stage >= 3) for (int i = tid; i < n; i += NT) Wb[i] = qnan;
         if (tid == 0) a.info[b] = code == kEigFailCode ? eig_fail_info(n) : code;
         return;
     }
 
     // ---- ascending rank of each eigenvalue
-    for (int j = tid; j < n; j += kNT) {
+    for (int j = tid; j < n; j += NT) {
         const double dj = order_key(v.dcd[j]);
         int r = 0;
         for (int k2 = 0; k2 < n; ++k2) {
@@ -503,7 +508,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             return (r == k + 1) ? c2(1.0, 0.0) : A[k + (size_t)r * ld];
         };
         // 1. Gram blocks: tiles (c, hr, hc) with hr <= hc, dealt to the warps
-        for (int t = warp; t < 3 * nblk; t += kNT / 32) {
+        for (int t = warp; t < 3 * nblk; t += NW) {
             const int c = t / 3, hh = t - 3 * c;
             const int hr = hh == 2 ? 1 : 0, hc = hh == 0 ? 0 : 1;
             double gr[2] = {0.0, 0.0}, gi[2] = {0.0, 0.0};
@@ -525,25 +530,25 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             }
         }
         // Z (real) into registers, then V = Z as complex in place
-        constexpr int ZR = (NMAX * NMAX + kNT - 1) / kNT;
+        constexpr int ZR = (NMAX * NMAX + NT - 1) / NT;
         double zr[ZR];
         const double* Z = reinterpret_cast<const double*>(B);
 #pragma unroll
         for (int u = 0; u < ZR; ++u) {
-            const int idx = tid + kNT * u, j = idx / n, i = idx - j * n;
+            const int idx = tid + NT * u, j = idx / n, i = idx - j * n;
             zr[u] = (idx < n * n) ? Z[i + (size_t)j * ld] : 0.0;
         }
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < ZR; ++u) {
-            const int idx = tid + kNT * u, j = idx / n, i = idx - j * n;
+            const int idx = tid + NT * u, j = idx / n, i = idx - j * n;
             if (idx < n * n) B[i + (size_t)j * ld] = c2(zr[u], 0.0);
         }
         // 2. T_c: lane l of warp c holds row l of T_c; column i needs
         // T(l, m < i) and G(m, i) (l <= m < i); every lane reads column i of
         // G before any lane overwrites it with column i of T.
-        if (warp < nblk) {
-            const int c = warp, l = lane;
+        for (int c = warp; c < nblk; c += NW) {
+            const int l = lane;
             const int mc = min(16, nref - 16 * c);
             double2 trow[16];
 #pragma unroll
@@ -570,9 +575,8 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             }
         }
         __syncthreads();
-        // 3. per-warp panels: columns [8p, 8p+8), p = warp (n <= 64)
-        const int p = warp;
-        if (8 * p < n) {
+        // 3. per-warp panels: columns [8p, 8p+8), p = warp, warp + NW, ...
+        for (int p = warp; 8 * p < n; p += NW) {
             const int jb = 8 * p + (lane >> 2);   // B-fragment column of this lane
             // W (16 x 8, accumulator layout: rows 8h + lane/4, columns
             // 2(lane%4) + e) -> B-fragment layout for k-step s: element
@@ -652,7 +656,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     __syncthreads();
     phase_mark(6);
     if (a.stage == 3) {
-        for (int jj = tr; jj < n; jj += 16) {
+        for (int jj = tr; jj < n; jj += TR) {
             double2* uo = Ub + (size_t)v.rank[jj] * n;
             for (int i = tc; i < n; i += 16) uo[i] = B[i + (size_t)jj * ld];
         }
@@ -662,16 +666,16 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     // ---- a6: U = X^H V, U(i, j) = sum_{k >= i} conj(X(k, i)) V(k, j), FP64
     // tensor-core tiles; U overwrites V after the barrier.
     {
-        constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + kNT / 32 - 1) / (kNT / 32);
+        constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + NW - 1) / NW;
         const int tn8 = (n + 7) >> 3;
         ZTiles<MAXT> acc;
-        ztiles_compute<MAXT>(acc, tn8, tn8,
+        ztiles_compute<MAXT, NT>(acc, tn8, tn8,
             [&](int i, int k) { return (i < n && k >= i && k < n) ? cconj(A[k + (size_t)i * ld]) : c2(0.0, 0.0); },
             [&](int k, int j) { return (k < n && j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0); },
             [&](int ti, int, int& k0, int& k1) { k0 = 8 * ti; k1 = n; },
             [](int, int) { return true; });
         __syncthreads();
-        ztiles_store<MAXT>(acc, tn8, tn8, [](int, int) { return true; },
+        ztiles_store<MAXT, NT>(acc, tn8, tn8, [](int, int) { return true; },
             [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
         __syncthreads();
         phase_mark(7);
@@ -689,10 +693,10 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         double2* Os = A;
         double* om = reinterpret_cast<double*>(v.pb);
         double* it = om + n;
-        for (int idx = tid; idx < 3 * n; idx += kNT) Os[idx] = __ldg(Ob + idx);
+        for (int idx = tid; idx < 3 * n; idx += NT) Os[idx] = __ldg(Ob + idx);
         const double q0 = __ldg(a.qhat + 3 * b), q1 = __ldg(a.qhat + 3 * b + 1), q2 = __ldg(a.qhat + 3 * b + 2);
         __syncthreads();
-        for (int jj = g; jj < n; jj += kNT / kG) {
+        for (int jj = g; jj < n; jj += NG) {
             const double lam = v.dcd[jj];
             double2 y0 = c2(0.0, 0.0), y1 = c2(0.0, 0.0), y2 = c2(0.0, 0.0);
             for (int i = q; i < n; i += kG) {
@@ -715,7 +719,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             }
         }
         __syncthreads();
-        for (int e = tid; e < a.ne; e += kNT) {
+        for (int e = tid; e < a.ne; e += NT) {
             const double E = __ldg(a.energies + e);
             double acc = 0.0;
             for (int jj = 0; jj < n; ++jj) {
@@ -729,7 +733,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         return;
     }
     // ---- a7: store U, column j to position rank[j]
-    for (int jj = tr; jj < n; jj += 16) {
+    for (int jj = tr; jj < n; jj += TR) {
         double2* uo = Ub + (size_t)v.rank[jj] * n;
         for (int i = tc; i < n; i += 16) uo[i] = B[i + (size_t)jj * ld];
     }

@@ -30,6 +30,7 @@ constexpr int kCtaMaxN = 64;
 constexpr int kCtaPreferredMaxN = 60;
 size_t cta_smem_bytes(int n);
 int cta_nmax_for(int n);
+int cta_threads_for(int nmax);   // threads per CTA of that row bound's kernel
 cudaError_t cta_set_attributes(int nmax, size_t smem);
 // `sigma`: H is the metric diag(I_{n/2}, -I_{n/2}) and is not read (H may be NULL).
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,

@@ -469,6 +469,7 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed
         p.regime = Regime::SmemCta;
         p.smem = cta_smem_bytes(n);
         p.nmax = cta_nmax_for(n);
+        p.threads = cta_threads_for(p.nmax);
         e = cta_set_attributes(p.nmax, (size_t)optin);
     } else if (!mixed && wide_ok && want == "smem-wide") {
         p.regime = Regime::SmemWide;
