@@ -124,7 +124,6 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
     s->tuning = tuning;
     s->cache = cache;
     s->bpb = 1;
-    (void)bpb_request;
     std::string err;
     std::string tuned_regime;
     e = with_device(device_id, [&]() -> cudaError_t {
@@ -149,12 +148,14 @@ sunny_geneig_solver_t create_impl(int n, int device_id, int bpb_request,
             s->tuned = true;
         }
         if (!sgeig::plain_plan(n, device_id, &s->plan, &err, mode == SUNNY_GENEIG_KERNEL_MIXED, regime,
-                               slots_per_sm)) {
+                               slots_per_sm, bpb_request)) {
             // a cached choice this build cannot run any more: the default choice
-            if (!s->tuned || !sgeig::plain_plan(n, device_id, &s->plan, &err, false, nullptr, 0))
+            if (!s->tuned || !sgeig::plain_plan(n, device_id, &s->plan, &err, false, nullptr, 0, bpb_request))
                 return cudaErrorInvalidValue;
             s->tuned = false;
         }
+        // batches per block: the pencils one CTA solves at a time
+        s->bpb = s->plan.regime == sgeig::Regime::SmemCta ? s->plan.teams : 1;
         if (s->plan.scratch_bytes) {
             cudaError_t ea = cudaMalloc(&s->scratch, s->plan.scratch_bytes);
             if (ea != cudaSuccess) { err = std::string("cudaMalloc scratch: ") + cudaGetErrorString(ea); return ea; }
@@ -357,7 +358,7 @@ sunny_geneig_status_t sunny_geneig_launch_sigma_intensity(sunny_geneig_solver_t 
                                                reinterpret_cast<const double*>(d_energies), n_energies, fwhm,
                                                reinterpret_cast<double*>(d_W), reinterpret_cast<double*>(d_spec),
                                                reinterpret_cast<int*>(d_info), batch_size,
-                                               reinterpret_cast<cudaStream_t>(stream));
+                                               reinterpret_cast<cudaStream_t>(stream), p.teams);
         });
         if (e != cudaSuccess) {
             set_error(std::string(fn) + ": kernel launch failed: " + cudaGetErrorString(e));

@@ -113,6 +113,24 @@ __host__ __device__ __forceinline__ double fast_rcp(double x) {
 #endif
 }
 
+// ---------------------------------------------------------------- teams
+// The NT threads that solve one pencil in a CTA of BLOCK threads: the whole
+// CTA when BLOCK == NT, else one of its BLOCK / NT teams of consecutive whole
+// warps (several pencils per CTA). team_sync is the team's barrier:
+// __syncthreads for a whole-CTA team, named barrier 1 + team otherwise
+// (barrier 0 stays the CTA's own).
+template <int NT, int BLOCK>
+__device__ __forceinline__ int team_tid() {
+    if constexpr (BLOCK == NT) return (int)threadIdx.x;
+    else return (int)(threadIdx.x % NT);
+}
+template <int NT, int BLOCK>
+__device__ __forceinline__ void team_sync() {
+    static_assert(NT % 32 == 0 && BLOCK % NT == 0 && BLOCK / NT <= 15, "team shape");
+    if constexpr (BLOCK == NT) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" :: "r"(1 + (int)(threadIdx.x / NT)), "n"(NT) : "memory");
+}
+
 // ---------------------------------------------------------------- constants
 // LAPACK dlamch convention: eps = 2^-53 (relative machine precision).
 constexpr double kEps    = 1.1102230246251565e-16;

@@ -53,12 +53,20 @@ template <> struct CtaShape<32> { static constexpr int nt = 128, minb = 4; };
 template <> struct CtaShape<40> { static constexpr int nt = kNT, minb = 3; };
 template <> struct CtaShape<48> { static constexpr int nt = 192, minb = 2; };
 
-template <int NMAX>
-__global__ void __launch_bounds__(CtaShape<NMAX>::nt, CtaShape<NMAX>::minb) geneig_cta_kernel(CtaArgs a) {
+// TEAMS pencils per CTA at a time (the reference's batches per block): the
+// CTA has TEAMS teams of CtaShape<NMAX>::nt threads, each with its own
+// barrier and shared-memory slice, team t taking pencils TEAMS * cta + t,
+// then a grid's stride on. TEAMS = 1 is the default launch.
+template <int NMAX, int TEAMS>
+__global__ void __launch_bounds__(CtaShape<NMAX>::nt * TEAMS, (CtaShape<NMAX>::minb + TEAMS - 1) / TEAMS)
+geneig_cta_kernel(CtaArgs a) {
+    constexpr int NT = CtaShape<NMAX>::nt;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     phase_start();
-    for (long long b = blockIdx.x; b < a.batch; b += gridDim.x)
-        cta_solve<NMAX, CtaShape<NMAX>::nt>(a, b, smem_raw);
+    const int t = TEAMS == 1 ? 0 : (int)(threadIdx.x / NT);
+    unsigned char* sm = smem_raw + (size_t)t * cta_team_bytes(a.n);
+    for (long long b = (long long)blockIdx.x * TEAMS + t; b < a.batch; b += (long long)gridDim.x * TEAMS)
+        cta_solve<NMAX, NT, NT * TEAMS>(a, b, sm);
 }
 
 }  // namespace
@@ -72,17 +80,22 @@ int cta_nmax_for(int n) {
 }
 
 using CtaKernelFn = void (*)(CtaArgs);
-static CtaKernelFn cta_kernel_for(int nmax) {
+static CtaKernelFn cta_kernel_for(int nmax, int teams) {
     switch (nmax) {
-        case 16: return geneig_cta_kernel<16>;
-        case 24: return geneig_cta_kernel<24>;
-        case 32: return geneig_cta_kernel<32>;
-        case 40: return geneig_cta_kernel<40>;
-        case 48: return geneig_cta_kernel<48>;
-        case 56: return geneig_cta_kernel<56>;
-        default: return geneig_cta_kernel<64>;
+        case 16: return teams == 4 ? geneig_cta_kernel<16, 4> : teams == 2 ? geneig_cta_kernel<16, 2>
+                                                                          : geneig_cta_kernel<16, 1>;
+        case 24: return teams == 2 ? geneig_cta_kernel<24, 2> : geneig_cta_kernel<24, 1>;
+        case 32: return teams == 2 ? geneig_cta_kernel<32, 2> : geneig_cta_kernel<32, 1>;
+        case 40: return geneig_cta_kernel<40, 1>;
+        case 48: return geneig_cta_kernel<48, 1>;
+        case 56: return geneig_cta_kernel<56, 1>;
+        default: return geneig_cta_kernel<64, 1>;
     }
 }
+
+int cta_max_teams(int nmax) { return nmax <= 16 ? 4 : nmax <= 32 ? 2 : 1; }
+
+size_t cta_teams_smem_bytes(int n, int teams) { return teams <= 1 ? cta_smem_bytes(n) : teams * cta_team_bytes(n); }
 
 int cta_threads_for(int nmax) {
     switch (nmax) {
@@ -99,15 +112,19 @@ int cta_threads_for(int nmax) {
 // `smem` is the per-CTA shared-memory limit; the kernel's own static shared
 // memory (profiling builds have some) comes off the dynamic allowance.
 cudaError_t cta_set_attributes(int nmax, size_t smem) {
-    cudaFuncAttributes fa{};
-    cudaError_t e = cudaFuncGetAttributes(&fa, cta_kernel_for(nmax));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(cta_kernel_for(nmax), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(smem - fa.sharedSizeBytes));
+    for (int teams = 1; teams <= cta_max_teams(nmax); teams *= 2) {
+        cudaFuncAttributes fa{};
+        cudaError_t e = cudaFuncGetAttributes(&fa, cta_kernel_for(nmax, teams));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(cta_kernel_for(nmax, teams), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(smem - fa.sharedSizeBytes));
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
-                       int* info, long long batch, cudaStream_t stream, bool sigma) {
+                       int* info, long long batch, cudaStream_t stream, bool sigma, int teams) {
     CtaArgs a;
     a.H = static_cast<const double2*>(H);
     a.S = static_cast<const double2*>(S);
@@ -124,14 +141,15 @@ cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, c
     a.spec = nullptr;
     a.ne = 0;
     a.gnorm = a.ginv2 = 0.0;
-    const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
-    cta_kernel_for(nmax)<<<(unsigned)grid, cta_threads_for(nmax), smem, stream>>>(a);
+    const long long ctas = (batch + teams - 1) / teams;
+    const long long grid = ctas < 0x7fffffffLL ? ctas : 0x7fffffffLL;
+    cta_kernel_for(nmax, teams)<<<(unsigned)grid, teams * cta_threads_for(nmax), smem, stream>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, const void* O, const double* qhat,
                                  const double* energies, int ne, double fwhm, double* W, double* spec, int* info,
-                                 long long batch, cudaStream_t stream) {
+                                 long long batch, cudaStream_t stream, int teams) {
     CtaArgs a;
     a.H = nullptr;
     a.S = static_cast<const double2*>(S);
@@ -151,8 +169,9 @@ cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, co
     const double sigma_e = fwhm / (2.0 * std::sqrt(2.0 * std::log(2.0)));
     a.gnorm = 1.0 / (sigma_e * std::sqrt(2.0 * M_PI));
     a.ginv2 = 1.0 / (2.0 * sigma_e * sigma_e);
-    const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
-    cta_kernel_for(nmax)<<<(unsigned)grid, cta_threads_for(nmax), smem, stream>>>(a);
+    const long long ctas = (batch + teams - 1) / teams;
+    const long long grid = ctas < 0x7fffffffLL ? ctas : 0x7fffffffLL;
+    cta_kernel_for(nmax, teams)<<<(unsigned)grid, teams * cta_threads_for(nmax), smem, stream>>>(a);
     return cudaGetLastError();
 }
 

@@ -66,6 +66,12 @@ __host__ __device__ inline size_t cta_vec_bytes(int n) {
            (size_t)dc_vec_ints(n) * 4 + (size_t)n * 4 + 8 * 4;
 }
 
+// Shared-memory bytes of one pencil's team (both matrices and the vector
+// area), rounded up to 16 so that consecutive teams stay aligned.
+__host__ __device__ inline size_t cta_team_bytes(int n) {
+    return ((size_t)2 * n * (n | 1) * 16 + cta_vec_bytes(n) + 15) & ~(size_t)15;
+}
+
 __device__ inline CtaVec cta_carve(unsigned char* p, int n) {
     CtaVec v;
     v.tau  = reinterpret_cast<double2*>(p);
@@ -105,9 +111,9 @@ struct ZTiles {
     double re[MAXT][2], im[MAXT][2];
 };
 
-template <int MAXT, int NT, class FA, class FB, class FK, class FKeep>
+template <int MAXT, int NT, int BLOCK, class FA, class FB, class FK, class FKeep>
 __device__ __forceinline__ void ztiles_compute(ZTiles<MAXT>& acc, int tm, int tn, FA fa, FB fb, FK kr, FKeep keep) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = team_tid<NT, BLOCK>() & 31, warp = team_tid<NT, BLOCK>() >> 5;
     constexpr int NW = NT / 32;
 #pragma unroll
     for (int u = 0; u < MAXT; ++u) {
@@ -131,9 +137,9 @@ __device__ __forceinline__ void ztiles_compute(ZTiles<MAXT>& acc, int tm, int tn
     }
 }
 
-template <int MAXT, int NT, class FKeep, class FPut>
+template <int MAXT, int NT, int BLOCK, class FKeep, class FPut>
 __device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, int tn, FKeep keep, FPut put) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = team_tid<NT, BLOCK>() & 31, warp = team_tid<NT, BLOCK>() >> 5;
     constexpr int NW = NT / 32;
 #pragma unroll
     for (int u = 0; u < MAXT; ++u) {
@@ -147,11 +153,12 @@ __device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, in
     }
 }
 
-// One pencil b, solved end to end by the whole CTA of NT threads (every
-// thread calls this with the same b and the dynamic shared memory of the
-// launch). NT >= 4 NMAX: the Cholesky gives each row a column group of
-// four lanes.
-template <int NMAX, int NT = kNT>
+// One pencil b, solved end to end by a team of NT threads (every thread of
+// the team calls this with the same b and the team's shared memory): the
+// whole CTA when BLOCK == NT, else one of the BLOCK / NT teams of a CTA of
+// BLOCK threads. NT >= 4 NMAX: the Cholesky gives each row a column group
+// of four lanes.
+template <int NMAX, int NT = kNT, int BLOCK = NT>
 __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, unsigned char* smem_raw) {
     constexpr int R = NMAX / kG;    // rows per lane in a column group
     constexpr int NW = NT / 32;     // warps
@@ -164,7 +171,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     double2* B = A + mat;
     CtaVec v = cta_carve(reinterpret_cast<unsigned char*>(B + mat), n);
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = team_tid<NT, BLOCK>(), lane = tid & 31, warp = tid >> 5;
     const int tr = tid >> 4, tc = tid & 15;
     const int g = tid >> 2, q = tid & 3;
     const unsigned gmask = 0xFu << (lane & ~3);
@@ -175,7 +182,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     double*  Wb = a.W + (size_t)b * n;
     double2* Ub = a.U + (size_t)b * nn;
 
-    __syncthreads();
+    team_sync<NT, BLOCK>();
     phase_mark(8);
     // ---- a1: load (rows by tc so that global reads are contiguous)
     for (int j = tr; j < n; j += TR)
@@ -199,7 +206,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     // barrier per step. The step loop is unrolled so that slot k is a
     // register known at compile time.
     int fail = 0;
-    __syncthreads();   // the loads above are complete
+    team_sync<NT, BLOCK>();   // the loads above are complete
     phase_mark(0);
     {
         const int i = g;
@@ -214,7 +221,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
 #pragma unroll
         for (int k = 0; k < NMAX; ++k) {
             if (k >= n) break;
-            __syncthreads();
+            team_sync<NT, BLOCK>();
             const double2* colk = v.colv + (k & 1) * n;
             const double2* rowk = v.rowv + (k & 1) * n;
             double2* coln = v.colv + ((k + 1) & 1) * n;
@@ -251,7 +258,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                 }
             }
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         if (!fail && a.stage >= 2 && i < n) {
             // X(i, j) = acc(i, j) r_i, X(i, i) = r_i, into A's lower triangle
 #pragma unroll
@@ -262,7 +269,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             }
         }
     }
-    __syncthreads();
+    team_sync<NT, BLOCK>();
     phase_mark(1);
     int code = fail ? n + fail : 0;   // zhegv: info = n + order of the failing minor
 
@@ -288,18 +295,18 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                     const double2 x = (i <= j) ? cconj(A[j + (size_t)i * ld]) : c2(0.0, 0.0);
                     B[i + (size_t)j * ld] = (i < m) ? x : c2(-x.x, -x.y);
                 }
-            __syncthreads();
+            team_sync<NT, BLOCK>();
         } else {
             ZTiles<MAXT> acc;
-            ztiles_compute<MAXT, NT>(acc, tn8, tn8,
+            ztiles_compute<MAXT, NT, BLOCK>(acc, tn8, tn8,
                 [&](int i, int k) { return (i < n && k < n) ? B[i + (size_t)k * ld] : c2(0.0, 0.0); },
                 [&](int k, int j) { return (j < n && k <= j) ? cconj(A[j + (size_t)k * ld]) : c2(0.0, 0.0); },
                 [&](int, int tj, int& k0, int& k1) { k0 = 0; k1 = min(n, 8 * tj + 8); },
                 [](int, int) { return true; });
-            __syncthreads();
-            ztiles_store<MAXT, NT>(acc, tn8, tn8, [](int, int) { return true; },
+            team_sync<NT, BLOCK>();
+            ztiles_store<MAXT, NT, BLOCK>(acc, tn8, tn8, [](int, int) { return true; },
                 [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
-            __syncthreads();
+            team_sync<NT, BLOCK>();
         }
         phase_mark(2);
         // ---- a4: C = X T, C(i, j) = sum_{k <= i} X(i, k) T(k, j); lower
@@ -307,13 +314,13 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         // C is exactly Hermitian.
         {
             ZTiles<MAXT> acc;
-            ztiles_compute<MAXT, NT>(acc, tn8, tn8,
+            ztiles_compute<MAXT, NT, BLOCK>(acc, tn8, tn8,
                 [&](int i, int k) { return (i < n && k <= i) ? A[i + (size_t)k * ld] : c2(0.0, 0.0); },
                 [&](int k, int j) { return (k < n && j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0); },
                 [&](int ti, int, int& k0, int& k1) { k0 = 0; k1 = min(n, 8 * ti + 8); },
                 [](int ti, int tj) { return ti >= tj; });
-            __syncthreads();
-            ztiles_store<MAXT, NT>(acc, tn8, tn8, [](int ti, int tj) { return ti >= tj; },
+            team_sync<NT, BLOCK>();
+            ztiles_store<MAXT, NT, BLOCK>(acc, tn8, tn8, [](int ti, int tj) { return ti >= tj; },
                 [&](int i, int j, double2 c) {
                     if (i < n && j < n && i >= j) {
                         if (i == j) c.y = 0.0;
@@ -321,7 +328,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                         B[j + (size_t)i * ld] = cconj(c);
                     }
                 });
-            __syncthreads();
+            team_sync<NT, BLOCK>();
             phase_mark(3);
         }
     }
@@ -372,7 +379,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             }
         };
         if (n >= 2 && warp == 0) reflect(0, v.vb);
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         for (int k = 0; k < n - 1; ++k) {
             double2* vk = (k & 1) ? v.vb2 : v.vb;
             double2* vn = (k & 1) ? v.vb : v.vb2;
@@ -390,7 +397,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                 }
                 dotp = warp_sum2(dotp);
                 if (lane == 0) v.wred[warp] = dotp;
-                __syncthreads();
+                team_sync<NT, BLOCK>();
             }
             // A22 -= v w^H + w v^H, w = p + alpha2 v, alpha2 = -tau/2 (p^H v)
             double2 alpha2 = c2(0.0, 0.0);
@@ -436,10 +443,10 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                     }
                 }
             }
-            __syncthreads();
+            team_sync<NT, BLOCK>();
         }
         if (tid == 0) v.d[n - 1] = B[(n - 1) + (size_t)(n - 1) * ld].x;
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(4);
         // ---- a5b: divide and conquer; Z (real) and its workspace in B
         DCShared dc;
@@ -449,13 +456,13 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         dc.w = v.dcd; dc.z = dc.w + n; dc.dl = dc.z + n; dc.zz = dc.dl + n; dc.zh = dc.zz + n;
         dc.rt = dc.zh + n; dc.rho = dc.rt + n; dc.scal = dc.rho + n;
         dc.org = v.dci; dc.nd = dc.org + n; dc.perm = dc.nd + n; dc.kcnt = dc.perm + n;
-        tridiag_dc<NT, NMAX>(n, dc);
+        tridiag_dc<NT, NMAX, BLOCK>(n, dc);
         if (tid == 0) {
             bool bad = false;
             for (int i = 0; i < n; ++i) bad |= !isfinite(dc.w[i]);
             v.ctl[4] = bad ? kEigFailCode : 0;
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(5);
         if (v.ctl[4]) code = v.ctl[4];
     }
@@ -538,7 +545,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             const int idx = tid + NT * u, j = idx / n, i = idx - j * n;
             zr[u] = (idx < n * n) ? Z[i + (size_t)j * ld] : 0.0;
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
 #pragma unroll
         for (int u = 0; u < ZR; ++u) {
             const int idx = tid + NT * u, j = idx / n, i = idx - j * n;
@@ -574,7 +581,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                 __syncwarp();
             }
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         // 3. per-warp panels: columns [8p, 8p+8), p = warp, warp + NW, ...
         for (int p = warp; 8 * p < n; p += NW) {
             const int jb = 8 * p + (lane >> 2);   // B-fragment column of this lane
@@ -653,7 +660,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
             }
         }
     }
-    __syncthreads();
+    team_sync<NT, BLOCK>();
     phase_mark(6);
     if (a.stage == 3) {
         for (int jj = tr; jj < n; jj += TR) {
@@ -669,15 +676,15 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         constexpr int MAXT = ((NMAX / 8) * (NMAX / 8) + NW - 1) / NW;
         const int tn8 = (n + 7) >> 3;
         ZTiles<MAXT> acc;
-        ztiles_compute<MAXT, NT>(acc, tn8, tn8,
+        ztiles_compute<MAXT, NT, BLOCK>(acc, tn8, tn8,
             [&](int i, int k) { return (i < n && k >= i && k < n) ? cconj(A[k + (size_t)i * ld]) : c2(0.0, 0.0); },
             [&](int k, int j) { return (k < n && j < n) ? B[k + (size_t)j * ld] : c2(0.0, 0.0); },
             [&](int ti, int, int& k0, int& k1) { k0 = 8 * ti; k1 = n; },
             [](int, int) { return true; });
-        __syncthreads();
-        ztiles_store<MAXT, NT>(acc, tn8, tn8, [](int, int) { return true; },
+        team_sync<NT, BLOCK>();
+        ztiles_store<MAXT, NT, BLOCK>(acc, tn8, tn8, [](int, int) { return true; },
             [&](int i, int j, double2 c) { if (i < n && j < n) B[i + (size_t)j * ld] = c; });
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(7);
     }
     if (a.stage == kStageIntensity) {
@@ -695,7 +702,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
         double* it = om + n;
         for (int idx = tid; idx < 3 * n; idx += NT) Os[idx] = __ldg(Ob + idx);
         const double q0 = __ldg(a.qhat + 3 * b), q1 = __ldg(a.qhat + 3 * b + 1), q2 = __ldg(a.qhat + 3 * b + 2);
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         for (int jj = g; jj < n; jj += NG) {
             const double lam = v.dcd[jj];
             double2 y0 = c2(0.0, 0.0), y1 = c2(0.0, 0.0), y2 = c2(0.0, 0.0);
@@ -718,7 +725,7 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
                 it[jj] = pos ? (yy - fma(qy.x, qy.x, qy.y * qy.y)) / lam : 0.0;
             }
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         for (int e = tid; e < a.ne; e += NT) {
             const double E = __ldg(a.energies + e);
             double acc = 0.0;

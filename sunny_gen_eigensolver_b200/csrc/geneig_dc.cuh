@@ -230,9 +230,9 @@ __host__ __device__ inline int secular_root(int i, int K, const double* dl, cons
 // the FP64 tensor cores (mma.m8n8k4.f64), one warp per tile, accumulators in
 // registers (n <= NMAX); all reads finish before the barrier, then the tiles
 // are written back to the gathered columns.
-template <int NT, int NMAX>
+template <int NT, int NMAX, int BLOCK = NT>
 __device__ __forceinline__ void dc_merge_top_regs(int n, const DCShared& s) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = team_tid<NT, BLOCK>() & 31, warp = team_tid<NT, BLOCK>() >> 5;
     constexpr int NW = NT / 32;
     const int K = s.kcnt[0];
     const int tm = (n + 7) >> 3, tn = (K + 7) >> 3;
@@ -253,7 +253,7 @@ __device__ __forceinline__ void dc_merge_top_regs(int n, const DCShared& s) {
                 : "+d"(acc[u][0]), "+d"(acc[u][1]) : "d"(av), "d"(bv));
         }
     }
-    __syncthreads();
+    team_sync<NT, BLOCK>();
 #pragma unroll
     for (int u = 0; u < MAXT; ++u) {
         const int t = warp + NW * u;
@@ -268,10 +268,10 @@ __device__ __forceinline__ void dc_merge_top_regs(int n, const DCShared& s) {
 // Phase E of a level of merges at most 4 * UMAX columns wide: four lanes per
 // row, lane q accumulating output columns j = q + 4u in registers. A row's
 // reads and writes stay within its quad, so no barrier is needed between them.
-template <int NT, int UMAX>
+template <int NT, int UMAX, int BLOCK = NT>
 __device__ __forceinline__ void dc_merge_rows_regs(int n, int half, int span, const DCShared& s) {
     for (int p0 = 0; p0 < 4 * n; p0 += NT) {
-        const int pidx = p0 + threadIdx.x;
+        const int pidx = p0 + team_tid<NT, BLOCK>();
         const int r = pidx >> 2, part = pidx & 3;
         const int a = (r < n) ? r - r % span : n;
         const bool active = r < n && a + half < n && s.kcnt[a] > 0;
@@ -300,9 +300,9 @@ __device__ __forceinline__ void dc_merge_rows_regs(int n, int half, int span, co
 // 16 x 16 warp tiles (2 x 2 mma.m8n8k4 tiles), rows outside [a, a+m) being
 // zero in those columns. Tiles are dealt round-robin to the warps across all
 // merges of the level; products go to Zo, then back into Z after a barrier.
-template <int NT>
+template <int NT, int BLOCK = NT>
 __device__ __forceinline__ void dc_merge_tiled(int n, int half, int span, const DCShared& s) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = team_tid<NT, BLOCK>() & 31, warp = team_tid<NT, BLOCK>() >> 5;
     constexpr int NW = NT / 32;
     int dealt = 0;
     for (int a = 0; a + half < n; a += span) {
@@ -353,9 +353,9 @@ __device__ __forceinline__ void dc_merge_tiled(int n, int half, int span, const 
         }
         dealt += T;
     }
-    __syncthreads();
+    team_sync<NT, BLOCK>();
     const int width = min(span, n);
-    for (int idx = threadIdx.x; idx < n * width; idx += NT) {
+    for (int idx = team_tid<NT, BLOCK>(); idx < n * width; idx += NT) {
         const int jj = idx / n, r = idx - jj * n;
         const int a = r - r % span;
         if (a + half >= n || jj >= s.kcnt[a]) continue;
@@ -366,9 +366,9 @@ __device__ __forceinline__ void dc_merge_tiled(int n, int half, int span, const 
 
 // All NT threads of the CTA call this. n >= 1. On return Z, w hold the
 // eigen-decomposition of the tridiagonal (d, e) given on entry.
-template <int NT, int NMAX>
+template <int NT, int NMAX, int BLOCK = NT>
 __device__ void tridiag_dc(int n, DCShared s) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = team_tid<NT, BLOCK>(), lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
 
     // ---- scale T by a power of two so that max |T_ij| is in [0.5, 1)
@@ -385,7 +385,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
             s.scal[0] = sc;
         }
     }
-    __syncthreads();
+    team_sync<NT, BLOCK>();
     const double sc = s.scal[0];
     // ---- scale, tear at every split, leaves: Z = I, w = d
     for (int i = tid; i < n; i += NT) {
@@ -394,13 +394,13 @@ __device__ void tridiag_dc(int n, DCShared s) {
         if (i < n - 1) di -= fabs(s.e[i] * sc);
         s.w[i] = di;
     }
-    __syncthreads();   // every unscaled e[] read above before it is scaled in place
+    team_sync<NT, BLOCK>();   // every unscaled e[] read above before it is scaled in place
     for (int i = tid; i < n - 1; i += NT) s.e[i] *= sc;
     for (int idx = tid; idx < n * n; idx += NT) {
         const int j = idx / n, i = idx - j * n;
         s.Z[i + j * s.ldz] = (i == j) ? 1.0 : 0.0;
     }
-    __syncthreads();
+    team_sync<NT, BLOCK>();
     phase_mark(10);
 
     for (int half = 1; half < n; half <<= 1) {
@@ -495,7 +495,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
                 s.rho[a] = rho;
             }
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(11);
         // ---- phase B: secular roots, four lanes per root (root slot = tid / 4)
         for (int p0 = 0; p0 < 4 * n; p0 += NT) {
@@ -515,7 +515,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
                 phase_level_max((unsigned)its);
             }
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(12);
         phase_level_flush(28);
         // ---- phase C: Loewner z-hat, four lanes per root
@@ -538,7 +538,7 @@ __device__ void tridiag_dc(int n, DCShared s) {
             W = lanes_prod<4>(W, qmask);
             if (qq == 0) s.zh[pidx] = copysign(sqrt(fmax(-W, 0.0)), s.zz[pidx]);
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(13);
         // ---- phase D: eigenvector columns of the rank-one problem (four lanes
         // per column), new eigenvalues
@@ -563,23 +563,23 @@ __device__ void tridiag_dc(int n, DCShared s) {
             for (int l = qq; l < K; l += 4) ucol[l] *= inv;
             if (qq == 0) s.w[s.nd[a + j]] = base + tj;
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(14);
         // ---- phase E: Z(:, nd) <- Z(:, nd) * U.
         if constexpr (NMAX > 0) {
-            if (span >= n) dc_merge_top_regs<NT, NMAX>(n, s);
-            else dc_merge_rows_regs<NT, pow2_below(NMAX) / 4>(n, half, span, s);
+            if (span >= n) dc_merge_top_regs<NT, NMAX, BLOCK>(n, s);
+            else dc_merge_rows_regs<NT, pow2_below(NMAX) / 4, BLOCK>(n, half, span, s);
         } else {
-            if (span <= 32) dc_merge_rows_regs<NT, 8>(n, half, span, s);
-            else dc_merge_tiled<NT>(n, half, span, s);
+            if (span <= 32) dc_merge_rows_regs<NT, 8, BLOCK>(n, half, span, s);
+            else dc_merge_tiled<NT, BLOCK>(n, half, span, s);
         }
-        __syncthreads();
+        team_sync<NT, BLOCK>();
         phase_mark(15);
     }
     // ---- back to the caller's units
     const double inv = 1.0 / sc;
     for (int i = tid; i < n; i += NT) s.w[i] *= inv;
-    __syncthreads();
+    team_sync<NT, BLOCK>();
 }
 
 }  // namespace sgeig

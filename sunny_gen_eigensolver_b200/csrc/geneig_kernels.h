@@ -30,11 +30,18 @@ constexpr int kCtaMaxN = 64;
 constexpr int kCtaPreferredMaxN = 60;
 size_t cta_smem_bytes(int n);
 int cta_nmax_for(int n);
-int cta_threads_for(int nmax);   // threads per CTA of that row bound's kernel
-cudaError_t cta_set_attributes(int nmax, size_t smem);
+int cta_threads_for(int nmax);   // threads per pencil (per team) of that row bound's kernel
+// Pencils per CTA at a time (teams) that row bound's kernels exist for: 4 for
+// nmax <= 16, 2 for nmax <= 32, else 1; and the dynamic shared memory of a
+// CTA of `teams` teams.
+int cta_max_teams(int nmax);
+size_t cta_teams_smem_bytes(int n, int teams);
+cudaError_t cta_set_attributes(int nmax, size_t smem);   // every teams form of the row bound
 // `sigma`: H is the metric diag(I_{n/2}, -I_{n/2}) and is not read (H may be NULL).
+// `teams`: pencils per CTA (1, or up to cta_max_teams(nmax)); smem from
+// cta_teams_smem_bytes.
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
-                       int* info, long long batch, cudaStream_t stream, bool sigma = false);
+                       int* info, long long batch, cudaStream_t stream, bool sigma = false, int teams = 1);
 
 // Spin-wave metric solve that reduces the eigenvectors to the spectrum
 // S(q, E) on the device (no U output): O is 3 x n complex per problem,
@@ -42,7 +49,7 @@ cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, c
 // problem; Gaussian broadening of full width at half maximum fwhm.
 cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, const void* O, const double* qhat,
                                  const double* energies, int ne, double fwhm, double* W, double* spec, int* info,
-                                 long long batch, cudaStream_t stream);
+                                 long long batch, cudaStream_t stream, int teams = 1);
 
 // Tiled kernel for the L2Slot regime (geneig_tiled.cu). A CTA's slot holds,
 // in double2 units, three n x ld complex matrices (four in the mixed form)
@@ -75,6 +82,7 @@ struct PlainPlan {
     size_t smem     = 0;      // dynamic shared memory per CTA
     Regime regime   = Regime::SmemCta;
     int    nmax     = 0;      // SmemCta: compile-time row bound of the register arrays
+    int    teams    = 1;      // SmemCta: pencils per CTA at a time (threads / teams each)
     int    slots    = 0;      // L2Slot: number of resident CTAs (= scratch slots)
     size_t scratch_bytes = 0; // L2Slot: bytes of device scratch needed
     bool   mixed    = false;  // mixed-precision form (always the L2Slot regime)
@@ -89,8 +97,12 @@ struct PlainPlan {
 // l2-slot CTAs per SM) request a configuration explicitly; a request that
 // cannot hold n fails with a message. NULL / "" and 0 keep the default
 // choice (or the SUNNY_GENEIG_REGIME / SUNNY_GENEIG_SLOTS_PER_SM overrides).
+// `pencils_per_cta` (the reference's batches per block request): 0 or 1
+// one pencil per CTA; 2 or 4 run that many pencils per CTA at a time where
+// the smem-cta kernel has that form (N <= 32 for 2, N <= 16 for 4), else
+// the largest form below the request (plan->teams says which).
 bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed = false,
-                const char* regime = nullptr, int slots_per_sm = 0);
+                const char* regime = nullptr, int slots_per_sm = 0, int pencils_per_cta = 0);
 
 // Enqueues one launch of `stage` (1..4) over `batch` matrices on `stream`.
 // `scratch` must hold plan.scratch_bytes when plan.regime == L2Slot.

@@ -415,7 +415,7 @@ int smem_cta_max_n() {
 }
 
 bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed, const char* regime,
-                int slots_per_sm) {
+                int slots_per_sm, int pencils_per_cta) {
     if (n < 1 || n > kMaxN) {
         *err = "matrix size out of range [1, " + std::to_string(kMaxN) + "]";
         return false;
@@ -467,9 +467,14 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed
     }
     if (!mixed && cta_ok && ((want.empty() && n <= kCtaPreferredMaxN) || want == "smem-cta")) {
         p.regime = Regime::SmemCta;
-        p.smem = cta_smem_bytes(n);
         p.nmax = cta_nmax_for(n);
-        p.threads = cta_threads_for(p.nmax);
+        int teams = 1;
+        while (teams * 2 <= pencils_per_cta && teams * 2 <= cta_max_teams(p.nmax) &&
+               cta_teams_smem_bytes(n, teams * 2) <= (size_t)optin)
+            teams *= 2;
+        p.teams = teams;
+        p.smem = cta_teams_smem_bytes(n, teams);
+        p.threads = teams * cta_threads_for(p.nmax);
         e = cta_set_attributes(p.nmax, (size_t)optin);
     } else if (!mixed && wide_ok && want == "smem-wide") {
         p.regime = Regime::SmemWide;
@@ -509,7 +514,7 @@ cudaError_t plain_launch(const PlainPlan& plan, int stage, const void* H, const 
     a.stage = stage;
     a.sigma = sigma ? 1 : 0;
     if (plan.regime == Regime::SmemCta)
-        return cta_launch(plan.n, plan.nmax, plan.smem, stage, H, S, W, U, info, batch, stream, sigma);
+        return cta_launch(plan.n, plan.nmax, plan.smem, stage, H, S, W, U, info, batch, stream, sigma, plan.teams);
     if (plan.regime == Regime::L2Slot)
         return tiled_launch(plan.n, plan.slots, plan.smem, stage, H, S, W, U, info, batch, scratch, stream, sigma,
                             plan.mixed, plan.refine_max);

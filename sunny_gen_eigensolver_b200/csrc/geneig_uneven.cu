@@ -10,6 +10,10 @@
 // per-pencil body as the size's own kernel (cta_solve / tiled_solve), so the
 // results are bitwise those of per-size launches. An l2-slot body uses the
 // CTA's own global-memory slot, sized for the largest l2-slot N of the mix.
+// Small pencils are solved several per CTA at a time: an item of N <= 16
+// goes to four 64-thread teams and one of N <= 32 to two 128-thread teams,
+// each team with its own barrier and shared-memory slice, taking the item's
+// pencils in turn (the thread counts of the sizes' own kernels).
 
 // The smem-cta bodies are called, each with its own register allocation
 // (inlining all of them with the tiled body into one function made the
@@ -20,6 +24,11 @@
 
 namespace sgeig {
 namespace {
+
+constexpr int kTeams16 = 4;   // 64-thread teams per CTA for N <= 16
+constexpr int kTeams32 = 2;   // 128-thread teams per CTA for N <= 32
+
+size_t team_slice(int n) { return (cta_smem_bytes(n) + 15) & ~(size_t)15; }
 
 struct UnevenGroup {
     const double2* H;
@@ -32,6 +41,7 @@ struct UnevenGroup {
     int n;
     int kind;               // 0..4: smem-cta row bound 16/32/48/56/64; 5: l2-slot
     int per_item;           // pencils per work item
+    size_t slice;           // kinds 0, 1: shared-memory bytes of one team
 };
 
 struct UnevenArgs {
@@ -72,8 +82,18 @@ __global__ void __launch_bounds__(256, 2) geneig_uneven_kernel(UnevenArgs a) {
             c.O = nullptr; c.qhat = nullptr; c.energies = nullptr; c.spec = nullptr; c.ne = 0;
             c.gnorm = 0.0; c.ginv2 = 0.0;
             switch (G.kind) {
-                case 0: for (long long b = b0; b < b1; ++b) cta::cta_solve<16>(c, b, smem_raw); break;
-                case 1: for (long long b = b0; b < b1; ++b) cta::cta_solve<32>(c, b, smem_raw); break;
+                case 0: {
+                    const int t = threadIdx.x / 64;
+                    for (long long b = b0 + t; b < b1; b += kTeams16)
+                        cta::cta_solve<16, 64, 256>(c, b, smem_raw + t * G.slice);
+                    break;
+                }
+                case 1: {
+                    const int t = threadIdx.x / 128;
+                    for (long long b = b0 + t; b < b1; b += kTeams32)
+                        cta::cta_solve<32, 128, 256>(c, b, smem_raw + t * G.slice);
+                    break;
+                }
                 case 2: for (long long b = b0; b < b1; ++b) cta::cta_solve<48>(c, b, smem_raw); break;
                 case 3: for (long long b = b0; b < b1; ++b) cta::cta_solve<56>(c, b, smem_raw); break;
                 default: for (long long b = b0; b < b1; ++b) cta::cta_solve<64>(c, b, smem_raw); break;
@@ -98,7 +118,10 @@ int uneven_kind(int n, bool l2slot) {
 }
 
 size_t uneven_smem_bytes(int n, int kind) {
-    return kind == 5 ? tiled_vec_bytes(n) : cta_smem_bytes(n);
+    return kind == 5 ? tiled_vec_bytes(n)
+         : kind == 0 ? kTeams16 * team_slice(n)
+         : kind == 1 ? kTeams32 * team_slice(n)
+         : cta_smem_bytes(n);
 }
 
 cudaError_t uneven_launch(const UnevenLaunch& L, unsigned long long* head, void* scratch, size_t slot_elems,
@@ -118,6 +141,7 @@ cudaError_t uneven_launch(const UnevenLaunch& L, unsigned long long* head, void*
         G.n = L.n[i];
         G.kind = L.kind[i];
         G.per_item = L.per_item[i] > 0 ? L.per_item[i] : 1;
+        G.slice = team_slice(G.n);
         G.first_item = first;
         first += (G.count + G.per_item - 1) / G.per_item;
     }

@@ -209,6 +209,36 @@ def test_batch_edges_and_determinism(cuda):
         assert torch.equal(Wx[0], W1[5]) and torch.equal(Ux[0], U1[5])
 
 
+@pytest.mark.parametrize("n,request_,expect", [(12, 4, 4), (16, 2, 2), (16, 8, 4), (24, 2, 2), (32, 4, 2),
+                                                (40, 2, 1), (54, 4, 1), (72, 4, 1)])
+def test_batches_per_block(cuda, n, request_, expect):
+    """batches_per_block_request > 1: several pencils per CTA (teams with their
+    own barriers) where the smem-cta kernel has that form; results, info
+    codes and the ragged last CTA equal the one-pencil-per-CTA launch bit for
+    bit (reference: src/unified/unified_solver.cpp:1021-1042 picks BPB)."""
+    import torch
+    from sunny_gen_eigensolver_b200 import Solver, to_colmajor
+    H, S = generators.baseline_problems(n, 37, seed=11)
+    S[5] = np.eye(n)
+    S[5, 2, 2] = -1.0                                   # info = n + 3
+    Ht = to_colmajor(torch.from_numpy(H).cuda())
+    St = to_colmajor(torch.from_numpy(S).cuda())
+    with Solver(n) as s1, Solver(n, bpb_request=request_) as s2:
+        assert s1.batches_per_block == 1
+        assert s2.batches_per_block == expect
+        assert s2.block_dim_x == expect * s1.block_dim_x
+        W1, U1, i1 = s1.run_kernel(Ht, St)
+        W2, U2, i2 = s2.run_kernel(Ht, St)
+        torch.cuda.synchronize()
+    assert torch.equal(i1, i2) and int(i2[5]) == n + 3
+    assert torch.equal(W1.nan_to_num(7.0), W2.nan_to_num(7.0))
+    assert torch.equal(U1.nan_to_num(7.0), U2.nan_to_num(7.0))
+    ok = i2.cpu().numpy() == 0
+    W = W2.cpu().numpy()
+    U = U2.transpose(-1, -2).cpu().numpy()
+    check_against_zhegv(H[ok], S[ok], W[ok], U[ok], i2.cpu().numpy()[ok])
+
+
 def test_abi_errors_on_gpu(cuda):
     import torch
     from sunny_gen_eigensolver_b200 import Solver, _native as nat
