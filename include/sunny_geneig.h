@@ -79,12 +79,12 @@ typedef enum {
 
 /* replaces src/common/c_api.h:50-55 (impl c_api.cpp:76-107).
  * Returns NULL on failure (message in sunny_geneig_last_error()).
- * batches_per_block_request: matrix pairs one CTA solves at a time. 0 or 1:
- * one per CTA (the default; small N already run several narrow CTAs per
- * SM). 2 or more: 2 for N <= 32, 4 for N <= 16 (the largest form at or
- * below the request that the shared-memory kernel has; 1 otherwise and in
- * the global-memory regime). sunny_geneig_batches_per_block reports the
- * choice. */
+ * batches_per_block_request: matrix pairs one CTA solves at a time. 0:
+ * automatic (4 for N <= 16, 2 for N = 25..32, else 1: the fastest measured
+ * on B200). 1: one per CTA. 2 or more: 2 for N <= 32, 4 for N <= 16 (the
+ * largest form at or below the request that the shared-memory kernel has;
+ * 1 otherwise and in the global-memory regime).
+ * sunny_geneig_batches_per_block reports the choice. */
 sunny_geneig_solver_t sunny_geneig_create(
     int                         n,
     int                         device_id,

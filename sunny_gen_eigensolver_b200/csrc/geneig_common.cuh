@@ -120,9 +120,9 @@ __host__ __device__ __forceinline__ double fast_rcp(double x) {
 // __syncthreads for a whole-CTA team, named barrier 1 + team otherwise
 // (barrier 0 stays the CTA's own).
 template <int NT, int BLOCK>
-__device__ __forceinline__ int team_tid() {
-    if constexpr (BLOCK == NT) return (int)threadIdx.x;
-    else return (int)(threadIdx.x % NT);
+__device__ __forceinline__ unsigned team_tid() {
+    if constexpr (BLOCK == NT) return threadIdx.x;
+    else return threadIdx.x % NT;
 }
 template <int NT, int BLOCK>
 __device__ __forceinline__ void team_sync() {

@@ -63,10 +63,14 @@ geneig_cta_kernel(CtaArgs a) {
     constexpr int NT = CtaShape<NMAX>::nt;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     phase_start();
-    const int t = TEAMS == 1 ? 0 : (int)(threadIdx.x / NT);
-    unsigned char* sm = smem_raw + (size_t)t * cta_team_bytes(a.n);
-    for (long long b = (long long)blockIdx.x * TEAMS + t; b < a.batch; b += (long long)gridDim.x * TEAMS)
-        cta_solve<NMAX, NT, NT * TEAMS>(a, b, sm);
+    if constexpr (TEAMS == 1) {
+        for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) cta_solve<NMAX, NT, NT>(a, b, smem_raw);
+    } else {
+        const int t = (int)(threadIdx.x / NT);
+        unsigned char* sm = smem_raw + (size_t)t * cta_team_bytes(a.n);
+        for (long long b = (long long)blockIdx.x * TEAMS + t; b < a.batch; b += (long long)gridDim.x * TEAMS)
+            cta_solve<NMAX, NT, NT * TEAMS>(a, b, sm);
+    }
 }
 
 }  // namespace
@@ -94,6 +98,12 @@ static CtaKernelFn cta_kernel_for(int nmax, int teams) {
 }
 
 int cta_max_teams(int nmax) { return nmax <= 16 ? 4 : nmax <= 32 ? 2 : 1; }
+
+// Default pencils per CTA, measured on B200 (solves/s at batch 65,536, one
+// pencil per CTA -> default): N=12 12.4 M -> 14.4 M, N=16 9.3 M -> 11.9 M
+// (4 teams of 64); N=32 2.2 M -> 3.0 M (2 of 128); N=24 stays at one
+// (4.4 M; 3.95 M with 2 teams).
+int cta_default_teams(int nmax) { return nmax <= 16 ? 4 : nmax == 32 ? 2 : 1; }
 
 size_t cta_teams_smem_bytes(int n, int teams) { return teams <= 1 ? cta_smem_bytes(n) : teams * cta_team_bytes(n); }
 

@@ -171,7 +171,9 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     double2* B = A + mat;
     CtaVec v = cta_carve(reinterpret_cast<unsigned char*>(B + mat), n);
 
-    const int tid = team_tid<NT, BLOCK>(), lane = tid & 31, warp = tid >> 5;
+    // (threadIdx.x read here directly: through team_tid the register
+    // allocation of the 56- and 64-row kernels spilled 300+ bytes)
+    const int tid = BLOCK == NT ? (int)threadIdx.x : (int)(threadIdx.x % NT), lane = tid & 31, warp = tid >> 5;
     const int tr = tid >> 4, tc = tid & 15;
     const int g = tid >> 2, q = tid & 3;
     const unsigned gmask = 0xFu << (lane & ~3);

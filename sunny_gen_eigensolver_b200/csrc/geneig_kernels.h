@@ -35,6 +35,7 @@ int cta_threads_for(int nmax);   // threads per pencil (per team) of that row bo
 // nmax <= 16, 2 for nmax <= 32, else 1; and the dynamic shared memory of a
 // CTA of `teams` teams.
 int cta_max_teams(int nmax);
+int cta_default_teams(int nmax);   // pencils per CTA when none is requested
 size_t cta_teams_smem_bytes(int n, int teams);
 cudaError_t cta_set_attributes(int nmax, size_t smem);   // every teams form of the row bound
 // `sigma`: H is the metric diag(I_{n/2}, -I_{n/2}) and is not read (H may be NULL).
@@ -97,10 +98,11 @@ struct PlainPlan {
 // l2-slot CTAs per SM) request a configuration explicitly; a request that
 // cannot hold n fails with a message. NULL / "" and 0 keep the default
 // choice (or the SUNNY_GENEIG_REGIME / SUNNY_GENEIG_SLOTS_PER_SM overrides).
-// `pencils_per_cta` (the reference's batches per block request): 0 or 1
-// one pencil per CTA; 2 or 4 run that many pencils per CTA at a time where
-// the smem-cta kernel has that form (N <= 32 for 2, N <= 16 for 4), else
-// the largest form below the request (plan->teams says which).
+// `pencils_per_cta` (the reference's batches per block request): 0 the
+// measured default (cta_default_teams), 1 one pencil per CTA, 2 or 4 that
+// many pencils per CTA at a time where the smem-cta kernel has that form
+// (N <= 32 for 2, N <= 16 for 4), else the largest form below the request
+// (plan->teams says which).
 bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed = false,
                 const char* regime = nullptr, int slots_per_sm = 0, int pencils_per_cta = 0);
 

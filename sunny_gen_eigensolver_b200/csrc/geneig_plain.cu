@@ -468,8 +468,9 @@ bool plain_plan(int n, int device, PlainPlan* plan, std::string* err, bool mixed
     if (!mixed && cta_ok && ((want.empty() && n <= kCtaPreferredMaxN) || want == "smem-cta")) {
         p.regime = Regime::SmemCta;
         p.nmax = cta_nmax_for(n);
+        const int want_teams = pencils_per_cta > 0 ? pencils_per_cta : cta_default_teams(p.nmax);
         int teams = 1;
-        while (teams * 2 <= pencils_per_cta && teams * 2 <= cta_max_teams(p.nmax) &&
+        while (teams * 2 <= want_teams && teams * 2 <= cta_max_teams(p.nmax) &&
                cta_teams_smem_bytes(n, teams * 2) <= (size_t)optin)
             teams *= 2;
         p.teams = teams;
@@ -625,10 +626,11 @@ extern "C" sunny_geneig_status_t sunny_geneig_launch_noalloc(int n, uintptr_t d_
     }
     if (n <= kCtaPreferredMaxN && cta_smem_bytes(n) <= (size_t)d->optin) {
         // the shared-memory kernel keeps everything on chip: no scratch at all
-        e = cta_launch(n, cta_nmax_for(n), cta_smem_bytes(n), 4, reinterpret_cast<const void*>(d_H),
+        const int nmax = cta_nmax_for(n), teams = cta_default_teams(nmax);
+        e = cta_launch(n, nmax, cta_teams_smem_bytes(n, teams), 4, reinterpret_cast<const void*>(d_H),
                        reinterpret_cast<const void*>(d_S), reinterpret_cast<double*>(d_W),
                        reinterpret_cast<void*>(d_U), reinterpret_cast<int*>(d_info), batch_size,
-                       reinterpret_cast<cudaStream_t>(stream), false);
+                       reinterpret_cast<cudaStream_t>(stream), false, teams);
         if (e != cudaSuccess) {
             api_set_error(std::string("sunny_geneig_launch_noalloc: kernel launch failed: ") + cudaGetErrorString(e));
             return SUNNY_GENEIG_LAUNCH_ERROR;

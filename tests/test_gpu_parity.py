@@ -223,7 +223,7 @@ def test_batches_per_block(cuda, n, request_, expect):
     S[5, 2, 2] = -1.0                                   # info = n + 3
     Ht = to_colmajor(torch.from_numpy(H).cuda())
     St = to_colmajor(torch.from_numpy(S).cuda())
-    with Solver(n) as s1, Solver(n, bpb_request=request_) as s2:
+    with Solver(n, bpb_request=1) as s1, Solver(n, bpb_request=request_) as s2:
         assert s1.batches_per_block == 1
         assert s2.batches_per_block == expect
         assert s2.block_dim_x == expect * s1.block_dim_x
