@@ -102,7 +102,9 @@ int cta_max_teams(int nmax) { return nmax <= 16 ? 4 : nmax <= 32 ? 2 : 1; }
 // Default pencils per CTA, measured on B200 (solves/s at batch 65,536, one
 // pencil per CTA -> default): N=12 12.4 M -> 14.4 M, N=16 9.3 M -> 11.9 M
 // (4 teams of 64); N=32 2.2 M -> 3.0 M (2 of 128); N=24 stays at one
-// (4.4 M; 3.95 M with 2 teams).
+// (4.4 M; 3.95 M with 2 teams). Two teams of the 48- and 56-row kernels
+// (384- and 512-thread CTAs, one per SM) were not kept: N=44 1.14 M vs
+// 1.16 M, N=48 1.05 M vs 0.98 M, N=54 810 K vs 836 K.
 int cta_default_teams(int nmax) { return nmax <= 16 ? 4 : nmax == 32 ? 2 : 1; }
 
 size_t cta_teams_smem_bytes(int n, int teams) { return teams <= 1 ? cta_smem_bytes(n) : teams * cta_team_bytes(n); }
