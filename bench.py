@@ -90,6 +90,10 @@ def parse():
     p.add_argument("--qmax", type=int, default=4096, help="serving: largest q-points per request")
     p.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
     p.add_argument("--slots", type=int, default=8, help="serving: requests in flight (streams)")
+    p.add_argument("--fourier", action="store_true",
+                   help="run the fused-assembly workload instead: S(q) built on the device from the Fourier "
+                        "terms of a seeded N/2-site spin-wave model, then the metric solve, in one launch")
+    p.add_argument("--bonds", type=int, default=120, help="fourier: exchange bonds of the model")
     return p.parse_args()
 
 
@@ -423,6 +427,153 @@ def run_e2e(args, torch, do_launch, H, S, W, U, info, dev, world, dist):
             "host_wall_s": time.perf_counter() - t0}
 
 
+def run_fourier(args):
+    """Fused dynamical-matrix assembly: per q-point, S(q) = sum_t coef_t
+    exp(2 pi i q . d_t) is built in shared memory from the terms of a seeded
+    spin-wave model (m = N/2 sites, --bonds exchange bonds, a field that gaps
+    every mode) and solved as the metric pencil H = diag(I, -I) in the same
+    launch (sunny_geneig_launch_fourier_sigma); S never exists in memory.
+    Against it: the unfused two-step path (the assembly as torch index_add
+    writing S to HBM, then sunny_geneig_launch_sigma reading it back)."""
+    import numpy as np
+    import torch
+    from sunny_gen_eigensolver_b200 import Solver, lswt
+    n, batch = args.n, args.batch
+    m = n // 2
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    model = lswt.random_model(m, args.bonds, seed=20261208)
+    rows, cols, coef, disp = lswt.fourier_terms(model)
+    start, c, d = lswt.pack_terms(n, rows, cols, coef, disp)
+    solver = Solver(n)
+    terms = solver.device_terms(start, c, d)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20261209)
+    q = (torch.rand((batch, 3), generator=gen, dtype=torch.float64, device=dev) - 0.5).contiguous()
+    W = torch.empty((batch, n), dtype=torch.float64, device=dev)
+    U = torch.empty((batch, n, n), dtype=torch.complex128, device=dev)
+    info = torch.empty((batch,), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    peak = measure_fp64_peak(torch, dev)
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3 / k
+
+    props = torch.cuda.get_device_properties(dev)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None)
+    with ClockSampler(uuid) as clk:
+        t_fused = timed(lambda: solver.launch_fourier_sigma(terms, q, W, U, info, stream), args.steps)
+    clocks = clk.summary()
+    bad = int((info != 0).sum().item())
+
+    # unfused: the same assembly in torch (S to HBM, column-major), then the metric solve
+    lower = np.asarray(rows) >= np.asarray(cols)
+    ent = torch.from_numpy((np.asarray(rows) + n * np.asarray(cols))[lower]).to(dev)
+    cf = torch.from_numpy(np.asarray(coef)[lower]).to(dev)
+    dp = torch.from_numpy(np.asarray(disp)[lower]).to(dev)
+    S = torch.zeros((batch, n, n), dtype=torch.complex128, device=dev)
+    W2, U2, info2 = torch.empty_like(W), torch.empty_like(U), torch.empty_like(info)
+    chunk = 8192
+
+    def assemble():
+        Sv = S.view(batch, n * n)
+        for c0 in range(0, batch, chunk):
+            x = 2 * np.pi * (q[c0:c0 + chunk] @ dp.T)
+            ph = torch.complex(torch.cos(x), torch.sin(x)) * cf
+            Sv[c0:c0 + chunk].zero_().index_add_(1, ent, ph)
+
+    def unfused():
+        assemble()
+        solver.launch_sigma(S, W2, U2, info2, stream)
+
+    t_unfused = timed(unfused, max(1, args.steps // 2))
+    # S is column-major with the lower triangle filled: mirror it for the host check
+    Sn = S.transpose(-1, -2)
+    Sfull = torch.tril(Sn) + torch.tril(Sn, -1).conj().transpose(-1, -2)
+    sig = torch.diag(torch.cat([torch.ones(m), -torch.ones(m)]).to(torch.complex128)).to(dev)
+    Hc = sig.expand(batch, n, n)
+    acc = {"failed_matrices": bad, "sorted": bool((W[:, 1:] >= W[:, :-1]).all().item()),
+           "max_eig_diff_fused_vs_unfused": float((W - W2).abs().max().item())}
+    acc.update(eig_err_vs_zhegv(Hc.transpose(-1, -2), Sfull.transpose(-1, -2), W))
+    res_max, orth_max = 0.0, 0.0
+    eye = torch.eye(n, dtype=torch.complex128, device=dev)
+    for c0 in range(0, batch, chunk):
+        sl = slice(c0, min(batch, c0 + chunk))
+        Un = U[sl].transpose(-1, -2)
+        Sl = Sfull[sl]
+        R = sig @ Un - (Sl @ Un) * W[sl, None, :].to(torch.complex128)
+        unorm_lb = torch.linalg.matrix_norm(Un) / n ** 0.5
+        res_max = max(res_max, float((torch.linalg.matrix_norm(R) / unorm_lb).max().item()))
+        orth_max = max(orth_max, float((Un.conj().transpose(-1, -2) @ Sl @ Un - eye).abs().amax().item()))
+    acc.update({"max_residual_upper_bound": res_max, "max_s_orth": orth_max})
+    del S, Sfull, Sn
+
+    # e2e through the C ABI: q in from pinned host memory, W, U, info out
+    qh = q.cpu().pin_memory()
+    Wh = torch.empty(W.shape, dtype=W.dtype).pin_memory()
+    Uh = torch.empty(U.shape, dtype=U.dtype).pin_memory()
+    ih = torch.empty(info.shape, dtype=info.dtype).pin_memory()
+    streams = [torch.cuda.Stream(dev) for _ in range(3)]
+
+    def step():
+        for k, off in enumerate(range(0, batch, chunk)):
+            sl = slice(off, min(batch, off + chunk))
+            st = streams[k % len(streams)]
+            with torch.cuda.stream(st):
+                q[sl].copy_(qh[sl], non_blocking=True)
+                solver.launch_fourier_sigma(terms, q[sl], W[sl], U[sl], info[sl], st)
+                Wh[sl].copy_(W[sl], non_blocking=True)
+                Uh[sl].copy_(U[sl], non_blocking=True)
+                ih[sl].copy_(info[sl], non_blocking=True)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cur = torch.cuda.current_stream(dev)
+    e2e_steps = max(3, args.steps // 2)
+    ev0.record(cur)
+    for st in streams:
+        st.wait_stream(cur)
+    for _ in range(e2e_steps):
+        step()
+    for st in streams:
+        cur.wait_stream(st)
+    ev1.record(cur)
+    torch.cuda.synchronize(dev)
+    el = ev0.elapsed_time(ev1) * 1e-3
+    e2e = {"value": batch * e2e_steps / el, "unit": "solves/s", "h2d_bytes_per_step": batch * 24,
+           "d2h_bytes_per_step": batch * (n * n * 16 + n * 8 + 4), "steps": e2e_steps, "chunk": chunk,
+           "streams": len(streams)}
+
+    achieved = flops_per_solve(n) * batch / t_fused / 1e12
+    out = {"metric": METRIC, "mode": "fourier", "value": batch / t_fused, "unit": "solves/s",
+           "ms_per_step": 1e3 * t_fused, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f64",
+           "data": "synthetic (seeded spin-wave model, uniform random q)",
+           "config": {"workload": f"N={n} spin-wave metric solve, S(q) assembled on the device "
+                                  f"({m} sites, {args.bonds} bonds, {int(c.shape[0])} lower-triangle terms)",
+                      "n": n, "batch": batch, "terms": int(c.shape[0])},
+           "unfused_solves_per_s": batch / t_unfused, "fused_vs_unfused": t_unfused / t_fused,
+           "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak, "traffic": None,
+                        "algorithmic_bytes_per_launch": batch * (24 + n * n * 16 + n * 8 + 4)},
+           "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps, "accuracy": acc,
+           "solver": {"regime": solver.regime, "block_dim_x": solver.block_dim_x}}
+    print(json.dumps(out), flush=True)
+    solver.close()
+
+
 def run_serving(args):
     """Serving workload: Poisson request arrivals, each request q log-uniform
     q-points of one N, admitted by a device-memory budget, overlapped on a
@@ -548,6 +699,8 @@ def main():
         run_serving(args)
     elif args.uneven:
         run_uneven(args)
+    elif args.fourier:
+        run_fourier(args)
     else:
         run_ours(args)
 

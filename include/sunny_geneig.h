@@ -215,6 +215,58 @@ sunny_geneig_status_t sunny_geneig_launch_sigma_intensity(
     int                   batch_size,
     uintptr_t             stream);
 
+/* Spin-wave metric solve with the metric-side matrix assembled on the device
+ * (Sunny's dynamical_matrix! step, which the reference's caller runs before
+ * sunny_geneig_launch: julia/SunnyGeneigBench/scripts/setup_sw08.jl:103),
+ * so that S never passes through device memory. For problem b with
+ * wavevector q = d_q[3b .. 3b+2] (reciprocal-lattice units), entry
+ * e = row + N col of the lower triangle (row >= col) of S is
+ *   S(q)_e = sum_{t = start[e]}^{start[e+1]-1} coef[t] exp(2 pi i q . disp[3t .. 3t+2]);
+ * upper-triangle entries are not read (S is Hermitian). Then exactly
+ * sunny_geneig_launch_sigma: H = diag(I_{N/2}, -I_{N/2}), W, U and info as
+ * for sunny_geneig_launch.
+ *   d_start   int32 N*N + 1, nondecreasing: entry e's terms are
+ *             [start[e], start[e+1]); indices outside [0, n_terms) are never
+ *             read (the sum is clipped to that range)
+ *   d_coef    complex128 n_terms; d_disp float64 3 per term (lattice units)
+ *   d_q       float64 3 per problem
+ * Needs a plain solver in the smem-cta regime (even N <= 64); INVALID_ARG
+ * otherwise. `sunny_gen_eigensolver_b200.lswt` builds the terms of a linear
+ * spin-wave model (sites, spin directions, exchange bonds, fields). */
+sunny_geneig_status_t sunny_geneig_launch_fourier_sigma(
+    sunny_geneig_solver_t solver,
+    uintptr_t             d_start,
+    uintptr_t             d_coef,
+    uintptr_t             d_disp,
+    int                   n_terms,
+    uintptr_t             d_q,
+    uintptr_t             d_W,
+    uintptr_t             d_U,
+    uintptr_t             d_info,
+    int                   batch_size,
+    uintptr_t             stream);
+
+/* The same assembly feeding the intensity form of
+ * sunny_geneig_launch_sigma_intensity (W and spec per problem, no U):
+ * assembly, solve and S(q, E) in one launch. */
+sunny_geneig_status_t sunny_geneig_launch_fourier_sigma_intensity(
+    sunny_geneig_solver_t solver,
+    uintptr_t             d_start,
+    uintptr_t             d_coef,
+    uintptr_t             d_disp,
+    int                   n_terms,
+    uintptr_t             d_q,
+    uintptr_t             d_O,
+    uintptr_t             d_qhat,
+    uintptr_t             d_energies,
+    int                   n_energies,
+    double                fwhm,
+    uintptr_t             d_W,
+    uintptr_t             d_spec,
+    uintptr_t             d_info,
+    int                   batch_size,
+    uintptr_t             stream);
+
 /* Create with an explicit execution configuration (no counterpart in the
  * reference; its NVRTC autotuner picked launch shapes inside create).
  * `regime` is "smem-cta", "smem-wide" or "l2-slot" (NULL or "" = the default

@@ -31,7 +31,8 @@ EXPORTS = (
     "sunny_geneig_regime_name", "sunny_geneig_selftest_reciprocal", "sunny_geneig_launch_noalloc",
     "sunny_geneig_launch_sigma", "sunny_geneig_create_config", "sunny_geneig_launch_sigma_intensity",
     "sunny_geneig_uneven_create", "sunny_geneig_uneven_launch", "sunny_geneig_uneven_destroy",
-    "sunny_geneig_uneven_shape",
+    "sunny_geneig_uneven_shape", "sunny_geneig_launch_fourier_sigma",
+    "sunny_geneig_launch_fourier_sigma_intensity",
 )
 
 _lib = None
@@ -71,6 +72,13 @@ def load() -> ctypes.CDLL:
     L.sunny_geneig_launch_sigma_intensity.argtypes = [c_void_p, c_size, c_size, c_size, c_size, c_int,
                                                       ctypes.c_double, c_size, c_size, c_size, c_int, c_size]
     L.sunny_geneig_launch_sigma_intensity.restype = c_int
+    L.sunny_geneig_launch_fourier_sigma.argtypes = [c_void_p, c_size, c_size, c_size, c_int, c_size, c_size,
+                                                    c_size, c_size, c_int, c_size]
+    L.sunny_geneig_launch_fourier_sigma.restype = c_int
+    L.sunny_geneig_launch_fourier_sigma_intensity.argtypes = [c_void_p, c_size, c_size, c_size, c_int, c_size,
+                                                              c_size, c_size, c_size, c_int, ctypes.c_double,
+                                                              c_size, c_size, c_size, c_int, c_size]
+    L.sunny_geneig_launch_fourier_sigma_intensity.restype = c_int
     p_int, p_size = ctypes.POINTER(c_int), ctypes.POINTER(c_size)
     L.sunny_geneig_uneven_create.argtypes = [c_int, p_int, p_int, p_int, c_int]
     L.sunny_geneig_uneven_create.restype = c_void_p

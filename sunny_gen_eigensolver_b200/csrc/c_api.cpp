@@ -244,6 +244,69 @@ void api_set_error(const std::string& msg) { set_error(msg); }
 void api_clear_error() { clear_error(); }
 }  // namespace sgeig
 
+namespace {
+// Shared body of the two fused-assembly entry points (d_O == 0: W and U).
+sunny_geneig_status_t fourier_impl(const char* fn, sunny_geneig_solver_t solver, uintptr_t d_start,
+                                   uintptr_t d_coef, uintptr_t d_disp, int n_terms, uintptr_t d_q, uintptr_t d_O,
+                                   uintptr_t d_qhat, uintptr_t d_energies, int n_energies, double fwhm,
+                                   uintptr_t d_W, uintptr_t d_U, uintptr_t d_spec, uintptr_t d_info,
+                                   int batch_size, uintptr_t stream) {
+    clear_error();
+    const bool intensity = d_O != 0 || d_spec != 0;
+    if (!solver) { set_error(std::string(fn) + ": solver is NULL"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (batch_size < 0) { set_error(std::string(fn) + ": batch_size < 0"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (n_terms < 0) { set_error(std::string(fn) + ": n_terms < 0"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (solver->n & 1) { set_error(std::string(fn) + ": n must be even"); return SUNNY_GENEIG_INVALID_ARG; }
+    if (solver->plan.regime != sgeig::Regime::SmemCta || solver->plan.mixed) {
+        set_error(std::string(fn) + ": needs a plain solver in the smem-cta regime (n <= " +
+                  std::to_string(sgeig::kCtaMaxN) + ")");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (intensity && (n_energies < 1 || !(fwhm > 0.0))) {
+        set_error(std::string(fn) + ": n_energies must be >= 1 and fwhm > 0");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (batch_size == 0) return SUNNY_GENEIG_OK;
+    if (!d_start || !d_q || !d_W || !d_info || (n_terms > 0 && (!d_coef || !d_disp)) ||
+        (intensity ? (!d_O || !d_qhat || !d_energies || !d_spec) : !d_U)) {
+        set_error(std::string(fn) + ": NULL device buffer");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    if (!aligned(d_start, 4) || !aligned(d_coef, 16) || !aligned(d_disp, 8) || !aligned(d_q, 8) ||
+        !aligned(d_W, 8) || !aligned(d_info, 4) || !aligned(d_U, 16) || !aligned(d_O, 16) ||
+        !aligned(d_qhat, 8) || !aligned(d_energies, 8) || !aligned(d_spec, 8)) {
+        set_error(std::string(fn) + ": misaligned device buffer (coef, U, O need 16 B; start, info 4 B; "
+                  "disp, q, W, qhat, energies, spec 8 B)");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    try {
+        const sgeig::PlainPlan& p = solver->plan;
+        sgeig::FourierTerms ft;
+        ft.start = reinterpret_cast<const int*>(d_start);
+        ft.coef = reinterpret_cast<const void*>(d_coef);
+        ft.disp = reinterpret_cast<const double*>(d_disp);
+        ft.nterms = n_terms;
+        cudaError_t e = with_device(solver->device, [&]() {
+            return sgeig::cta_launch_fourier(p.n, p.nmax, ft, reinterpret_cast<const double*>(d_q),
+                                             intensity ? reinterpret_cast<const void*>(d_O) : nullptr,
+                                             reinterpret_cast<const double*>(d_qhat),
+                                             reinterpret_cast<const double*>(d_energies), n_energies, fwhm,
+                                             reinterpret_cast<double*>(d_W), reinterpret_cast<void*>(d_U),
+                                             reinterpret_cast<double*>(d_spec), reinterpret_cast<int*>(d_info),
+                                             batch_size, reinterpret_cast<cudaStream_t>(stream));
+        });
+        if (e != cudaSuccess) {
+            set_error(std::string(fn) + ": kernel launch failed: " + cudaGetErrorString(e));
+            return SUNNY_GENEIG_LAUNCH_ERROR;
+        }
+    } catch (...) {
+        set_error(std::string("unknown C++ exception in ") + fn);
+        return SUNNY_GENEIG_LAUNCH_ERROR;
+    }
+    return SUNNY_GENEIG_OK;
+}
+}  // namespace
+
 #pragma GCC visibility push(default)
 extern "C" {
 
@@ -318,6 +381,28 @@ sunny_geneig_status_t sunny_geneig_launch_sigma(sunny_geneig_solver_t solver, ui
                                                 uintptr_t d_U, uintptr_t d_info, int batch_size, uintptr_t stream) {
     return launch_impl(solver, 4, 0, d_S, d_W, d_U, d_info, batch_size, stream, "sunny_geneig_launch_sigma",
                        true);
+}
+
+sunny_geneig_status_t sunny_geneig_launch_fourier_sigma(sunny_geneig_solver_t solver, uintptr_t d_start,
+                                                        uintptr_t d_coef, uintptr_t d_disp, int n_terms,
+                                                        uintptr_t d_q, uintptr_t d_W, uintptr_t d_U,
+                                                        uintptr_t d_info, int batch_size, uintptr_t stream) {
+    return fourier_impl("sunny_geneig_launch_fourier_sigma", solver, d_start, d_coef, d_disp, n_terms, d_q, 0, 0,
+                        0, 0, 0.0, d_W, d_U, 0, d_info, batch_size, stream);
+}
+
+sunny_geneig_status_t sunny_geneig_launch_fourier_sigma_intensity(
+    sunny_geneig_solver_t solver, uintptr_t d_start, uintptr_t d_coef, uintptr_t d_disp, int n_terms, uintptr_t d_q,
+    uintptr_t d_O, uintptr_t d_qhat, uintptr_t d_energies, int n_energies, double fwhm, uintptr_t d_W,
+    uintptr_t d_spec, uintptr_t d_info, int batch_size, uintptr_t stream) {
+    const char* fn = "sunny_geneig_launch_fourier_sigma_intensity";
+    if (solver && batch_size > 0 && (!d_O || !d_spec)) {
+        clear_error();
+        set_error(std::string(fn) + ": NULL device buffer");
+        return SUNNY_GENEIG_INVALID_ARG;
+    }
+    return fourier_impl(fn, solver, d_start, d_coef, d_disp, n_terms, d_q, d_O, d_qhat, d_energies,
+                        n_energies, fwhm, d_W, 0, d_spec, d_info, batch_size, stream);
 }
 
 sunny_geneig_status_t sunny_geneig_launch_sigma_intensity(sunny_geneig_solver_t solver, uintptr_t d_S,

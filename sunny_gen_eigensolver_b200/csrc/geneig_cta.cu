@@ -73,6 +73,16 @@ geneig_cta_kernel(CtaArgs a) {
     }
 }
 
+// S assembled on the device from Fourier terms (one pencil per CTA).
+template <int NMAX>
+__global__ void __launch_bounds__(CtaShape<NMAX>::nt, CtaShape<NMAX>::minb)
+geneig_cta_fourier_kernel(CtaArgs a, CtaFourier f) {
+    constexpr int NT = CtaShape<NMAX>::nt;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    phase_start();
+    for (long long b = blockIdx.x; b < a.batch; b += gridDim.x) cta_solve<NMAX, NT, NT, true>(a, b, smem_raw, &f);
+}
+
 }  // namespace
 
 size_t cta_smem_bytes(int n) { return (size_t)2 * n * (n | 1) * 16 + cta_vec_bytes(n); }
@@ -94,6 +104,20 @@ static CtaKernelFn cta_kernel_for(int nmax, int teams) {
         case 48: return geneig_cta_kernel<48, 1>;
         case 56: return geneig_cta_kernel<56, 1>;
         default: return geneig_cta_kernel<64, 1>;
+    }
+}
+
+// The assembled-S (Fourier) form, one pencil per CTA.
+using CtaFourierKernelFn = void (*)(CtaArgs, CtaFourier);
+static CtaFourierKernelFn cta_fourier_kernel_for(int nmax) {
+    switch (nmax) {
+        case 16: return geneig_cta_fourier_kernel<16>;
+        case 24: return geneig_cta_fourier_kernel<24>;
+        case 32: return geneig_cta_fourier_kernel<32>;
+        case 40: return geneig_cta_fourier_kernel<40>;
+        case 48: return geneig_cta_fourier_kernel<48>;
+        case 56: return geneig_cta_fourier_kernel<56>;
+        default: return geneig_cta_fourier_kernel<64>;
     }
 }
 
@@ -124,6 +148,14 @@ int cta_threads_for(int nmax) {
 // `smem` is the per-CTA shared-memory limit; the kernel's own static shared
 // memory (profiling builds have some) comes off the dynamic allowance.
 cudaError_t cta_set_attributes(int nmax, size_t smem) {
+    {
+        cudaFuncAttributes fa{};
+        cudaError_t e = cudaFuncGetAttributes(&fa, cta_fourier_kernel_for(nmax));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(cta_fourier_kernel_for(nmax), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(smem - fa.sharedSizeBytes));
+        if (e != cudaSuccess) return e;
+    }
     for (int teams = 1; teams <= cta_max_teams(nmax); teams *= 2) {
         cudaFuncAttributes fa{};
         cudaError_t e = cudaFuncGetAttributes(&fa, cta_kernel_for(nmax, teams));
@@ -137,7 +169,7 @@ cudaError_t cta_set_attributes(int nmax, size_t smem) {
 
 cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, const void* S, double* W, void* U,
                        int* info, long long batch, cudaStream_t stream, bool sigma, int teams) {
-    CtaArgs a;
+    CtaArgs a{};
     a.H = static_cast<const double2*>(H);
     a.S = static_cast<const double2*>(S);
     a.W = W;
@@ -162,7 +194,7 @@ cudaError_t cta_launch(int n, int nmax, size_t smem, int stage, const void* H, c
 cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, const void* O, const double* qhat,
                                  const double* energies, int ne, double fwhm, double* W, double* spec, int* info,
                                  long long batch, cudaStream_t stream, int teams) {
-    CtaArgs a;
+    CtaArgs a{};
     a.H = nullptr;
     a.S = static_cast<const double2*>(S);
     a.W = W;
@@ -187,6 +219,41 @@ cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, co
     return cudaGetLastError();
 }
 
+
+cudaError_t cta_launch_fourier(int n, int nmax, const FourierTerms& ft, const double* q,
+                               const void* O, const double* qhat, const double* energies, int ne, double fwhm,
+                               double* W, void* U, double* spec, int* info, long long batch, cudaStream_t stream) {
+    CtaArgs a{};
+    a.W = W;
+    a.U = static_cast<double2*>(U);
+    a.info = info;
+    a.batch = batch;
+    a.n = n;
+    a.ld = n | 1;
+    a.sigma = 1;
+    CtaFourier f{};
+    f.start = ft.start;
+    f.coef = static_cast<const double2*>(ft.coef);
+    f.disp = ft.disp;
+    f.q = q;
+    f.nterms = ft.nterms;
+    if (O) {
+        a.stage = kStageIntensity;
+        a.O = static_cast<const double2*>(O);
+        a.qhat = qhat;
+        a.energies = energies;
+        a.spec = spec;
+        a.ne = ne;
+        const double sigma_e = fwhm / (2.0 * std::sqrt(2.0 * std::log(2.0)));
+        a.gnorm = 1.0 / (sigma_e * std::sqrt(2.0 * M_PI));
+        a.ginv2 = 1.0 / (2.0 * sigma_e * sigma_e);
+    } else {
+        a.stage = 4;
+    }
+    const long long grid = batch < 0x7fffffffLL ? batch : 0x7fffffffLL;
+    cta_fourier_kernel_for(nmax)<<<(unsigned)grid, cta_threads_for(nmax), cta_smem_bytes(n), stream>>>(a, f);
+    return cudaGetLastError();
+}
 
 }  // namespace sgeig
 

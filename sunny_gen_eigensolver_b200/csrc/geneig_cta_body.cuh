@@ -44,6 +44,17 @@ struct CtaArgs {
     double         ginv2;    // 1 / (2 sigma^2)
 };
 
+// S assembled on the device instead of loaded (the FS form of cta_solve):
+// S(q)_e = sum_{t in [start[e], start[e+1])} coef[t] exp(2 pi i q . disp[3t..3t+2])
+// for the lower-triangle entries e = row + n col (row >= col), q = q[3b..3b+2].
+struct CtaFourier {
+    const int*     start;   // n*n + 1
+    const double2* coef;
+    const double*  disp;
+    const double*  q;
+    int            nterms;  // terms are read only from [0, nterms)
+};
+
 struct CtaVec {
     double2* tau;   // n   Householder scalars
     double2* vb;    // n   Householder vector of even steps
@@ -157,9 +168,12 @@ __device__ __forceinline__ void ztiles_store(const ZTiles<MAXT>& acc, int tm, in
 // the team calls this with the same b and the team's shared memory): the
 // whole CTA when BLOCK == NT, else one of the BLOCK / NT teams of a CTA of
 // BLOCK threads. NT >= 4 NMAX: the Cholesky gives each row a column group
-// of four lanes.
-template <int NMAX, int NT = kNT, int BLOCK = NT>
-__device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, unsigned char* smem_raw) {
+// of four lanes. FS: S is assembled from the Fourier terms `fs` instead of
+// loaded (a separate instantiation, so that the plain solve's register
+// allocation is untouched).
+template <int NMAX, int NT = kNT, int BLOCK = NT, bool FS = false>
+__device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, unsigned char* smem_raw,
+                                                const CtaFourier* fs = nullptr) {
     constexpr int R = NMAX / kG;    // rows per lane in a column group
     constexpr int NW = NT / 32;     // warps
     constexpr int NG = NT / kG;     // column groups
@@ -187,11 +201,41 @@ __device__ SGEIG_CTA_BODY_INLINE void cta_solve(const CtaArgs& a, long long b, u
     team_sync<NT, BLOCK>();
     phase_mark(8);
     // ---- a1: load (rows by tc so that global reads are contiguous)
-    for (int j = tr; j < n; j += TR)
-        for (int i = tc; i < n; i += 16) {
-            A[i + (size_t)j * ld] = __ldg(Sb + i + (size_t)j * n);
-            if (!a.sigma) B[i + (size_t)j * ld] = __ldg(Hb + i + (size_t)j * n);
+    if constexpr (FS) {
+        // S(q) from its Fourier terms, lower triangle (the only part the
+        // Cholesky reads); the terms are shared by all pencils (L1/L2-resident).
+        // Term values first, one term per thread (coalesced, independent
+        // loads), into B, which the metric solve leaves free until a3; then
+        // each lower entry sums its terms in table order.
+        const double q0 = __ldg(fs->q + 3 * b), q1 = __ldg(fs->q + 3 * b + 1), q2 = __ldg(fs->q + 3 * b + 2);
+        const int nt = fs->nterms;
+        auto term = [&](int t) {
+            const double x = fma(q0, __ldg(fs->disp + 3 * t),
+                             fma(q1, __ldg(fs->disp + 3 * t + 1), q2 * __ldg(fs->disp + 3 * t + 2)));
+            double sn, cs;
+            sincospi(2.0 * x, &sn, &cs);
+            return cmul(__ldg(fs->coef + t), c2(cs, sn));
+        };
+        const bool staged = nt <= n * ld;
+        if (staged) {
+            for (int t = tid; t < nt; t += NT) B[t] = term(t);
+            team_sync<NT, BLOCK>();
         }
+        for (int idx = tid; idx < n * n; idx += NT) {
+            const int j = idx / n, i = idx - j * n;
+            if (i < j) continue;
+            double2 acc = c2(0.0, 0.0);
+            const int t1 = min(__ldg(fs->start + idx + 1), nt);
+            for (int t = max(__ldg(fs->start + idx), 0); t < t1; ++t) acc = cadd(acc, staged ? B[t] : term(t));
+            A[i + (size_t)j * ld] = acc;
+        }
+    } else {
+        for (int j = tr; j < n; j += TR)
+            for (int i = tc; i < n; i += 16) {
+                A[i + (size_t)j * ld] = __ldg(Sb + i + (size_t)j * n);
+                if (!a.sigma) B[i + (size_t)j * ld] = __ldg(Hb + i + (size_t)j * n);
+            }
+    }
     if (tid < 8) v.ctl[tid] = 0;
 
     // ---- a2: Cholesky S = L L^H fused with X = L^-1, in registers.

@@ -52,6 +52,23 @@ cudaError_t cta_launch_intensity(int n, int nmax, size_t smem, const void* S, co
                                  const double* energies, int ne, double fwhm, double* W, double* spec, int* info,
                                  long long batch, cudaStream_t stream, int teams = 1);
 
+// Spin-wave metric solve with S assembled on the device from Fourier terms
+// (no S in memory): entry e = row + n col of the lower triangle is
+// S(q)_e = sum_{t in [start[e], start[e+1])} coef[t] exp(2 pi i q . disp[3t..3t+2]),
+// start int32[n*n + 1], coef complex128, disp 3 doubles per term, q 3
+// doubles per problem. O == NULL: W and U as cta_launch (stage 4); else the
+// intensity form of cta_launch_intensity (W and spec, no U). One pencil per
+// CTA (its own kernel instantiation), dynamic smem cta_smem_bytes(n).
+struct FourierTerms {
+    const int*    start  = nullptr;
+    const void*   coef   = nullptr;
+    const double* disp   = nullptr;
+    int           nterms = 0;   // terms outside [0, nterms) are never read
+};
+cudaError_t cta_launch_fourier(int n, int nmax, const FourierTerms& ft, const double* q,
+                               const void* O, const double* qhat, const double* energies, int ne, double fwhm,
+                               double* W, void* U, double* spec, int* info, long long batch, cudaStream_t stream);
+
 // Tiled kernel for the L2Slot regime (geneig_tiled.cu). A CTA's slot holds,
 // in double2 units, three n x ld complex matrices (four in the mixed form)
 // and an n x ld real one (at least 16 n complex); the mixed form adds an

@@ -177,6 +177,73 @@ class Solver:
         if st != nat.STATUS_OK:
             raise RuntimeError(f"sunny_geneig_launch_sigma_intensity failed (status={st}): {nat.last_error()}")
 
+    @staticmethod
+    def _fourier_args(terms, q, batch):
+        start, coef, disp = terms
+        checks = ((start, None, torch.int32), (coef, None, torch.complex128), (disp, None, torch.float64),
+                  (q, (batch, 3), torch.float64))
+        for t, shape, dt in checks:
+            if (t.dtype != dt or not t.is_cuda or not t.is_contiguous()
+                    or (shape is not None and tuple(t.shape) != shape)):
+                raise ValueError(f"fourier terms / q: expected contiguous CUDA tensors of {dt}")
+        nt = coef.shape[0]
+        if tuple(disp.shape) != (nt, 3):
+            raise ValueError("disp must have shape (n_terms, 3)")
+        return start.data_ptr(), coef.data_ptr(), disp.data_ptr(), int(nt), q.data_ptr()
+
+    def device_terms(self, start, coef, disp, device=None):
+        """Moves a packed term table (lswt.pack_terms) to the device."""
+        dev = device if device is not None else torch.device("cuda", self.device_id)
+        if start.shape[0] != self.n * self.n + 1:
+            raise ValueError(f"start must have n*n + 1 = {self.n * self.n + 1} entries")
+        return (torch.as_tensor(start, dtype=torch.int32).to(dev).contiguous(),
+                torch.as_tensor(coef, dtype=torch.complex128).to(dev).contiguous(),
+                torch.as_tensor(disp, dtype=torch.float64).reshape(-1, 3).to(dev).contiguous())
+
+    def launch_fourier_sigma(self, terms, q, W, U, info, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """Metric solve with S(q) assembled on the device from Fourier terms
+        (sunny_geneig_launch_fourier_sigma): terms = (start, coef, disp) from
+        device_terms, q (batch, 3) float64; W (batch, n), U (batch, n, n)
+        column-major, info (batch,) as for `launch`. S is never in memory."""
+        batch = q.shape[0]
+        n = self.n
+        for t, shape, dt in ((W, (batch, n), torch.float64), (U, (batch, n, n), torch.complex128),
+                             (info, (batch,), torch.int32)):
+            if tuple(t.shape) != shape or t.dtype != dt or not t.is_cuda or not t.is_contiguous():
+                raise ValueError(f"expected a contiguous CUDA tensor {shape} of {dt}")
+        p_start, p_coef, p_disp, nt, p_q = self._fourier_args(terms, q, batch)
+        s = stream if stream is not None else torch.cuda.current_stream(q.device)
+        st = self._lib.sunny_geneig_launch_fourier_sigma(self.handle, p_start, p_coef, p_disp, nt, p_q,
+                                                         W.data_ptr(), U.data_ptr(), info.data_ptr(), int(batch),
+                                                         s.cuda_stream)
+        if st != nat.STATUS_OK:
+            raise RuntimeError(f"sunny_geneig_launch_fourier_sigma failed (status={st}): {nat.last_error()}")
+
+    def launch_fourier_sigma_intensity(self, terms, q, O, qhat, energies, fwhm: float, W, spec, info,
+                                       stream: Optional[torch.cuda.Stream] = None) -> None:
+        """Assembly, metric solve and intensities in one launch
+        (sunny_geneig_launch_fourier_sigma_intensity); the arguments after q
+        are those of `launch_sigma_intensity`."""
+        batch = q.shape[0]
+        n = self.n
+        checks = ((O, (batch, n, 3), torch.complex128), (qhat, (batch, 3), torch.float64),
+                  (W, (batch, n), torch.float64), (info, (batch,), torch.int32))
+        for t, shape, dt in checks:
+            if tuple(t.shape) != shape or t.dtype != dt or not t.is_cuda or not t.is_contiguous():
+                raise ValueError(f"expected a contiguous CUDA tensor {shape} of {dt}")
+        ne = energies.shape[0]
+        if (energies.dtype != torch.float64 or not energies.is_cuda or not energies.is_contiguous()
+                or tuple(spec.shape) != (batch, ne) or spec.dtype != torch.float64 or not spec.is_contiguous()):
+            raise ValueError("energies (ne,) and spec (batch, ne) must be contiguous float64 CUDA tensors")
+        p_start, p_coef, p_disp, nt, p_q = self._fourier_args(terms, q, batch)
+        s = stream if stream is not None else torch.cuda.current_stream(q.device)
+        st = self._lib.sunny_geneig_launch_fourier_sigma_intensity(
+            self.handle, p_start, p_coef, p_disp, nt, p_q, O.data_ptr(), qhat.data_ptr(), energies.data_ptr(),
+            int(ne), float(fwhm), W.data_ptr(), spec.data_ptr(), info.data_ptr(), int(batch), s.cuda_stream)
+        if st != nat.STATUS_OK:
+            raise RuntimeError(
+                f"sunny_geneig_launch_fourier_sigma_intensity failed (status={st}): {nat.last_error()}")
+
     def run_kernel(self, H: torch.Tensor, S: torch.Tensor, W: Optional[torch.Tensor] = None,
                    U: Optional[torch.Tensor] = None, info: Optional[torch.Tensor] = None,
                    stream: Optional[torch.cuda.Stream] = None) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
