@@ -105,3 +105,12 @@ def test_fourier_entry_points_reject_null_handle():
     st = L.sunny_geneig_launch_fourier_sigma_intensity(None, 0, 0, 0, 0, 0, 0, 0, 0, 8, ctypes.c_double(0.1),
                                                       0, 0, 0, 4, 0)
     assert st == nat.STATUS_INVALID_ARG and "NULL" in nat.last_error()
+
+
+def test_random_model_is_seeded_and_packs_empty_tables():
+    a = lswt.fourier_terms(lswt.random_model(5, 12, seed=7))
+    b = lswt.fourier_terms(lswt.random_model(5, 12, seed=7))
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    start, c, d = lswt.pack_terms(6, np.zeros(0, int), np.zeros(0, int), np.zeros(0, complex), np.zeros((0, 3)))
+    assert start.shape == (37,) and (start == 0).all() and c.shape == (0,) and d.shape == (0, 3)
