@@ -1,6 +1,10 @@
 // Batched generalized Hermitian-definite eigensolver, shared-memory regime
-// (N <= 64): one CTA (64 to 256 threads by N) holds one matrix pair in
-// shared memory and solves it end to end; CTAs loop over the batch.
+// (N <= 64): a team of NT threads (64 to 256 by N) holds one matrix pair in
+// shared memory and solves it end to end; a CTA is one team or, with
+// several pencils per CTA, up to four, each with its own named barrier and
+// shared-memory slice; CTAs loop over the batch. A second kernel form
+// assembles S(q) from Fourier terms in the load stage (the metric solve of
+// a spin-wave dynamical matrix that never exists in memory).
 //
 // Stage chain (reference: src/unified/kernel_source.hpp:233-276):
 //   a1  load S -> A, H -> B                                   (:233-242)
